@@ -1,0 +1,321 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 statevector engine on its headline workload.
+
+Workload (one step): 30-qubit complex128 brick-wall circuit of depth 40 (U3 on every
+qubit, CNOT brick, a 29-control multi-controlled Z on the all-ones pattern and an
+RZZ(gamma) on a seeded random pair per layer; angles from SplitMix64 seed 3030),
+run from |0...0> with fusion, followed by countsAll(8192) with seed 42.
+Metric: gate-level amplitude updates per second (1.643e12 per step).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs N independent replicas (one process per GPU under torchrun, weak
+scaling); the state vector of one circuit does not shard without an exchange.
+`--impl reference` times the CPU restatement of the reference engine (the Java
+engine cannot run here) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "amp-updates/s (30q c128 brick-wall depth 40 + MCZ29 + RZZ, fused, countsAll 8192)"
+UNIT = "amp-updates/s"
+CPU_QUBITS = 26   # bounded CPU sample: same generator, fewer qubits / layers
+CPU_LAYERS = 8
+
+
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--qubits", type=int, default=30)
+    ap.add_argument("--layers", type=int, default=40)
+    ap.add_argument("--shots", type=int, default=8192)
+    ap.add_argument("--tile-qubits", type=int, default=0)
+    ap.add_argument("--sweep-budget", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        if self.path and os.path.exists(self.path):
+            for line in open(self.path):
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    try:
+                        rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+                    except ValueError:
+                        pass
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        load = [r for r in rows if r[2] > 200.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in load for k, v in enumerate(r[3]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in load),
+                "sm_max_mhz": max(r[1] for r in rows), "reasons": reasons,
+                "samples": len(rows), "power_w_max": max(r[2] for r in rows)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+def ncu_traffic() -> dict:
+    """DRAM bytes per sweep launch from the committed ncu summary, when present."""
+    p = ROOT / "profiles" / "sweep_kernel_traffic.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (the oracle restatement of the reference engine, OpenMP)
+# ---------------------------------------------------------------------------
+def cpu_baseline(seconds_budget: float = 30.0) -> dict:
+    from oracle import oracle as O
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import serialize_circuit
+
+    cores = len(os.sched_getaffinity(0))
+    c = W.brickwall_circuit(CPU_QUBITS, CPU_LAYERS, seed=3030, mcz=True, rzz=True)
+    ops, n_ops = serialize_circuit(c)
+    st = O.initial_state(CPU_QUBITS)
+    t0 = time.perf_counter()
+    rc, _ = O.run(CPU_QUBITS, ops, n_ops, st)
+    dt = time.perf_counter() - t0
+    assert rc == 0
+    return {"value": W.amp_updates(c) / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "seconds": dt,
+            "sample": (f"C restatement of StatevectorEngine (per-gate sweeps, OpenMP {cores} threads, "
+                       f"-O2) on the same brick-wall generator at {CPU_QUBITS} qubits x {CPU_LAYERS} "
+                       f"layer(s) ({n_ops} ops); the Java engine is unavailable on this host")}
+
+
+def run_reference(args, rank: int) -> None:
+    if rank != 0:
+        return
+    from statecraft_b200 import workloads as W
+
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    for _ in range(args.warmup):
+        cpu_baseline()
+    vals = []
+    t_all = 0.0
+    for _ in range(args.steps):
+        r = cpu_baseline()
+        vals.append(r["value"])
+        t_all += r["seconds"]
+    value = float(np.median(vals))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"brick-wall U3+CNOT+MCZ+RZZ, {CPU_QUBITS} qubits x {CPU_LAYERS} "
+                                   f"layer(s) per step (bounded CPU sample of the 30q x 40 workload)",
+                       "qubits": CPU_QUBITS, "layers": CPU_LAYERS},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# the B200 engine
+# ---------------------------------------------------------------------------
+def main(argv=None) -> int:
+    args = parse_args(argv)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return 0
+
+    import torch
+    import torch.distributed as dist
+
+    from statecraft_b200 import _abi as A
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import (B200Config, MeasurementInstruction, NativeContext,
+                                        SimulationRequest, StatevectorB200Engine,
+                                        serialize_circuit)
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+
+    n, layers, shots = args.qubits, args.layers, args.shots
+    circuit = W.brickwall_circuit(n, layers, seed=3030, mcz=True, rzz=True)
+    ops, n_ops = serialize_circuit(circuit)
+    updates = W.amp_updates(circuit)
+    qubits = list(range(n))
+    cfg = B200Config(device=local_rank, timing=True, tile_qubits=args.tile_qubits,
+                     sweep_budget=args.sweep_budget)
+    ctx = NativeContext(cfg)
+    stream = torch.cuda.ExternalStream(ctx.lib.sc_stream(ctx.handle), device=local_rank)
+
+    def step():
+        ctx.run_ops(n, ops, n_ops)
+        return ctx.sample(qubits, shots, 42)
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    ctx.reset_kernel_stats()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        start.record(stream)
+        for _ in range(args.steps):
+            outcomes = step()
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    dev_ms = start.elapsed_time(end)
+    stats = ctx.kernel_stats()
+    plan = ctx.plan_stats()
+    t = torch.tensor([dev_ms], device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    max_ms = float(t.item())
+    value = world * updates * args.steps / (max_ms / 1e3)
+    launches = sum(v["launches"] for v in stats.values())
+    ctx.close()
+
+    # e2e through the public engine API: host circuit in, host histogram out
+    e2e = None
+    if not args.no_e2e:
+        engine = StatevectorB200Engine(B200Config(device=local_rank, tile_qubits=args.tile_qubits,
+                                                  sweep_budget=args.sweep_budget))
+        req = SimulationRequest.zeroState(circuit).withMeasurement(
+            MeasurementInstruction.countsAll(shots).withSeed(42), False)
+        engine.simulate(req)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            res = engine.simulate(req)
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        te = torch.tensor([e2e_s], device="cuda")
+        if world > 1:
+            dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        e2e_s = float(te.item())
+        assert sum(res.measurement.counts.values()) == shots
+        e2e = {"value": world * updates * args.steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": n_ops * 280, "d2h_bytes_per_step": shots * 4,
+               "seconds_per_step": e2e_s / args.steps}
+        engine.close()
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs")
+    sw = stats.get("sweep", {"launches": 0, "ms": 0.0, "bytes": 0.0})
+    roofline = None
+    if sw["launches"] > 0 and sw["ms"] > 0:
+        per_launch_bytes = sw["bytes"] / sw["launches"]
+        avg_s = sw["ms"] / sw["launches"] / 1e3
+        achieved = per_launch_bytes / avg_s / 1e9
+        peak = hbm if hbm else 6650.0
+        tr = ncu_traffic()
+        traffic = None
+        if tr.get("bytes_per_amplitude"):
+            traffic = tr["bytes_per_amplitude"] * (2 ** n)
+        roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "peak_source": "measured" if hbm else "fallback",
+                    "kernel": "k_sweep (fused tile sweep)",
+                    "algorithmic_bytes_per_launch": per_launch_bytes,
+                    "avg_launch_ms": sw["ms"] / sw["launches"],
+                    "share_of_step": sw["ms"] / max(dev_ms, 1e-9)}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"brick-wall U3+CNOT+MCZ{n - 1}+RZZ, {n} qubits x {layers} layers, "
+                                   f"countsAll({shots}) seed 42, c128",
+                       "qubits": n, "layers": layers, "shots": shots, "angle_seed": 3030,
+                       "replicas": world,
+                       "l2": f"state {2 ** n * 16 / 2 ** 30:.0f} GiB per GPU exceeds the 126 MB L2",
+                       "amp_updates_per_step": updates,
+                       "sweeps_per_step": plan["sweeps"], "gates_per_step": plan["gates"],
+                       "stages_per_step": plan["stages"]},
+            "gpu_launches": launches,
+            "kernel_stats": stats,
+            "roofline": roofline,
+            "e2e": e2e,
+            "clocks": clk.summary()}
+    if world == 1 and not args.no_cpu_baseline:
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+        line["cpu_baseline"] = cpu_baseline()
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

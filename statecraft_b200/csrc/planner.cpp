@@ -1,0 +1,397 @@
+// Gate normalisation and the fusion planner (host side).
+//
+// The reference engine applies one full-state sweep per operation
+// (StatevectorEngine.java:90-151).  Here the op list is normalised into dense,
+// permutation and diagonal gates, a commutation-aware dependency DAG is built,
+// and gates are packed greedily into tile sweeps: each sweep streams every
+// amplitude through shared memory / registers once and applies every gate whose
+// dense qubits lie in the sweep's tile, in an order that respects the DAG.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "sc_internal.h"
+
+namespace sc {
+
+static inline bool czero(double re, double im) { return re == 0.0 && im == 0.0; }
+
+double gate_cost(const PGate& g) {
+  switch (g.kind) {
+    case PK_DENSE1: return 8.0;   // 2 complex MACs per amplitude
+    case PK_DENSE2: return 16.0;  // 4 complex MACs per amplitude
+    case PK_DIAG1:
+    case PK_DIAG2: return 3.0;    // 1 complex multiply + bit tests
+    default: return 0.5;          // register selects
+  }
+}
+
+uint64_t dense_mask(const PGate& g) {
+  switch (g.kind) {
+    case PK_DENSE1:
+    case PK_X: return 1ULL << g.q0;
+    case PK_DENSE2:
+    case PK_SWAP: return (1ULL << g.q0) | (1ULL << g.q1);
+    default: return 0;
+  }
+}
+
+uint64_t touch_mask(const PGate& g) {
+  uint64_t m = g.cmask | (1ULL << g.q0);
+  if (g.kind == PK_DENSE2 || g.kind == PK_SWAP || g.kind == PK_DIAG2) m |= 1ULL << g.q1;
+  return m;
+}
+
+static void rotation(int kind, double a, double* g) {
+  const double half = a / 2.0;
+  const double c = std::cos(half), s = std::sin(half);
+  std::memset(g, 0, 8 * sizeof(double));
+  if (kind == SC_OP_RX) {
+    g[0] = c; g[3] = -s; g[5] = -s; g[6] = c;
+  } else {  // RY
+    g[0] = c; g[2] = -s; g[4] = s; g[6] = c;
+  }
+}
+
+bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate* out,
+                  bool* produced) {
+  *produced = false;
+  PGate g;
+  std::memset(&g, 0, sizeof g);
+  g.q1 = -1;
+  auto angle = [&]() {
+    return (op.param >= 0 && params && op.param < n_params) ? params[op.param] : op.m[0];
+  };
+  switch (op.kind) {
+    case SC_OP_MEASURE: return true;
+    case SC_OP_SINGLE:
+    case SC_OP_MULTI: {
+      const double* m = op.m;
+      g.q0 = op.q0;
+      g.cmask = (op.kind == SC_OP_MULTI) ? op.mask : 0;
+      const bool off_zero = czero(m[2], m[3]) && czero(m[4], m[5]);
+      const bool diag_zero = czero(m[0], m[1]) && czero(m[6], m[7]);
+      if (off_zero) {
+        g.kind = PK_DIAG1;
+        g.m[0] = m[0]; g.m[1] = m[1]; g.m[2] = m[6]; g.m[3] = m[7];
+      } else if (diag_zero && m[2] == 1.0 && m[3] == 0.0 && m[4] == 1.0 && m[5] == 0.0) {
+        g.kind = PK_X;
+      } else {
+        g.kind = PK_DENSE1;
+        std::memcpy(g.m, m, 8 * sizeof(double));
+      }
+      break;
+    }
+    case SC_OP_CNOT:
+      g.kind = PK_X;
+      g.q0 = op.q1;
+      g.cmask = 1ULL << op.q0;
+      break;
+    case SC_OP_TWO: {
+      g.q0 = op.q0;
+      g.q1 = op.q1;
+      bool diagonal = true;
+      for (int r = 0; r < 4 && diagonal; ++r)
+        for (int c = 0; c < 4; ++c)
+          if (r != c && !czero(op.m[2 * (4 * r + c)], op.m[2 * (4 * r + c) + 1])) {
+            diagonal = false;
+            break;
+          }
+      if (diagonal) {
+        g.kind = PK_DIAG2;
+        for (int k = 0; k < 4; ++k) {
+          g.m[2 * k] = op.m[2 * (5 * k)];
+          g.m[2 * k + 1] = op.m[2 * (5 * k) + 1];
+        }
+      } else {
+        g.kind = PK_DENSE2;
+        std::memcpy(g.m, op.m, 32 * sizeof(double));
+      }
+      break;
+    }
+    case SC_OP_DIAG2:
+      g.kind = PK_DIAG2;
+      g.q0 = op.q0;
+      g.q1 = op.q1;
+      std::memcpy(g.m, op.m, 8 * sizeof(double));
+      break;
+    case SC_OP_SWAP:
+      g.kind = PK_SWAP;
+      g.q0 = op.q0;
+      g.q1 = op.q1;
+      break;
+    case SC_OP_RX:
+    case SC_OP_RY:
+      g.kind = PK_DENSE1;
+      g.q0 = op.q0;
+      rotation(op.kind, angle(), g.m);
+      break;
+    case SC_OP_RZ: {
+      const double h = angle() / 2.0;
+      g.kind = PK_DIAG1;
+      g.q0 = op.q0;
+      g.m[0] = std::cos(-h); g.m[1] = std::sin(-h);
+      g.m[2] = std::cos(h); g.m[3] = std::sin(h);
+      break;
+    }
+    case SC_OP_RZZ: {
+      const double h = angle() / 2.0;
+      g.kind = PK_DIAG2;
+      g.q0 = op.q0;
+      g.q1 = op.q1;
+      const double cr = std::cos(-h), ci = std::sin(-h), pr = std::cos(h), pi = std::sin(h);
+      g.m[0] = cr; g.m[1] = ci; g.m[2] = pr; g.m[3] = pi;
+      g.m[4] = pr; g.m[5] = pi; g.m[6] = cr; g.m[7] = ci;
+      break;
+    }
+    default: return false;
+  }
+  *produced = true;
+  *out = g;
+  return true;
+}
+
+// ---------------------------------------------------------------------------
+// planner
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Dag {
+  std::vector<int32_t> dep_off;  // CSR
+  std::vector<int32_t> deps;
+};
+
+Dag build_dag(const std::vector<PGate>& gates, int n) {
+  const int G = (int)gates.size();
+  Dag d;
+  d.dep_off.assign(G + 1, 0);
+  std::vector<int32_t> last_dense(n, -1);
+  std::vector<std::vector<int32_t>> diag_since(n);
+  std::vector<int32_t> tmp;
+  for (int g = 0; g < G; ++g) {
+    const uint64_t dm = dense_mask(gates[g]);
+    const uint64_t dg = touch_mask(gates[g]) & ~dm;
+    tmp.clear();
+    for (uint64_t m = dm; m; m &= m - 1) {
+      const int q = __builtin_ctzll(m);
+      if (last_dense[q] >= 0) tmp.push_back(last_dense[q]);
+      tmp.insert(tmp.end(), diag_since[q].begin(), diag_since[q].end());
+    }
+    for (uint64_t m = dg; m; m &= m - 1) {
+      const int q = __builtin_ctzll(m);
+      if (last_dense[q] >= 0) tmp.push_back(last_dense[q]);
+    }
+    for (uint64_t m = dm; m; m &= m - 1) {
+      const int q = __builtin_ctzll(m);
+      last_dense[q] = g;
+      diag_since[q].clear();
+    }
+    for (uint64_t m = dg; m; m &= m - 1) diag_since[__builtin_ctzll(m)].push_back(g);
+    std::sort(tmp.begin(), tmp.end());
+    tmp.erase(std::unique(tmp.begin(), tmp.end()), tmp.end());
+    d.deps.insert(d.deps.end(), tmp.begin(), tmp.end());
+    d.dep_off[g + 1] = (int32_t)d.deps.size();
+  }
+  return d;
+}
+
+inline int popc(uint64_t x) { return __builtin_popcountll(x); }
+
+}  // namespace
+
+Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
+  Plan plan;
+  const int G = (int)gates.size();
+  plan.n_gates = G;
+  if (G == 0) return plan;
+
+  // a stage must hold both qubits of a two-qubit gate
+  const int NR = std::min(std::max(pp.nr, 2), n);
+  const int L0 = std::min(pp.low_qubits, n);
+  int T = std::min(pp.tile_qubits, n);
+  // keep at least 2^8 tiles per sweep when the state allows it
+  if (n - T < 8) T = n - 8;
+  // the tile must hold a stage's registers and two high qubits (a 2-qubit gate)
+  T = std::max(T, std::min(n, std::max(NR, L0 + 2)));
+  const int L = std::min(L0, T);
+  const int h = T - L;
+  const uint64_t low_qmask = (L >= 64) ? ~0ULL : ((1ULL << L) - 1ULL);
+  const bool high_edges = h >= NR;  // first/last stage can use only high positions
+
+  Dag dag = build_dag(gates, n);
+  std::vector<int32_t> when(G, -1);
+  std::vector<int32_t> idx_in_sweep(G, -1);
+  int first = 0;
+  int sweep_id = 0;
+  std::vector<int32_t> list;
+  std::vector<char> staged;
+
+  while (first < G) {
+    uint64_t H = 0;
+    int hcount = 0;
+    double used = 0.0;
+    list.clear();
+    for (int g = first; g < G; ++g) {
+      if (when[g] >= 0) continue;
+      bool ok = true;
+      for (int k = dag.dep_off[g]; k < dag.dep_off[g + 1]; ++k)
+        if (when[dag.deps[k]] < 0) { ok = false; break; }
+      if (!ok) continue;
+      const uint64_t need = dense_mask(gates[g]) & ~low_qmask & ~H;
+      const int c = popc(need);
+      if (hcount + c > h) continue;
+      const double cost = gate_cost(gates[g]);
+      if (pp.budget >= 0 && !list.empty() && used + cost > pp.budget) break;
+      if ((int)list.size() >= pp.max_gates) break;
+      H |= need;
+      hcount += c;
+      used += cost;
+      when[g] = sweep_id;
+      list.push_back(g);
+    }
+    // pad the high set to exactly h qubits so every sweep tile has 2^T amplitudes
+    for (int q = L; q < n && hcount < h; ++q)
+      if (!((H >> q) & 1ULL)) { H |= 1ULL << q; ++hcount; }
+
+    SwSweep sw;
+    std::memset(&sw, 0, sizeof sw);
+    sw.T = T; sw.L = L; sw.h = h; sw.nr = NR;
+    sw.tiles = 1LL << (n - T);
+    int pos_of[64];
+    for (int q = 0; q < 64; ++q) pos_of[q] = -1;
+    for (int q = 0; q < L; ++q) pos_of[q] = q;
+    {
+      int k = 0;
+      for (uint64_t m = H; m; m &= m - 1) {
+        const int q = __builtin_ctzll(m);
+        sw.hq[k] = q;
+        pos_of[q] = L + k;
+        ++k;
+      }
+    }
+    const uint32_t high_pos = (T >= 32 ? 0xFFFFFFFFu : ((1u << T) - 1u)) & ~((1u << L) - 1u);
+
+    // ---- stages -----------------------------------------------------------
+    for (size_t i = 0; i < list.size(); ++i) idx_in_sweep[list[i]] = (int32_t)i;
+    staged.assign(list.size(), 0);
+    size_t remaining = list.size();
+    sw.s0 = (int32_t)plan.stages.size();
+    std::vector<std::pair<uint32_t, std::vector<int32_t>>> stage_list;
+    while (remaining > 0 || stage_list.empty()) {
+      const bool first_stage = stage_list.empty();
+      uint32_t R = 0;
+      std::vector<int32_t> sg;
+      for (size_t i = 0; i < list.size(); ++i) {
+        if (staged[i]) continue;
+        const int g = list[i];
+        bool ok = true;
+        for (int k = dag.dep_off[g]; k < dag.dep_off[g + 1]; ++k) {
+          const int dpd = dag.deps[k];
+          if (when[dpd] == sweep_id && !staged[idx_in_sweep[dpd]]) { ok = false; break; }
+        }
+        if (!ok) continue;
+        uint32_t need = 0;
+        for (uint64_t m = dense_mask(gates[g]); m; m &= m - 1)
+          need |= 1u << pos_of[__builtin_ctzll(m)];
+        need &= ~R;
+        if (first_stage && high_edges && (need & ~high_pos)) continue;
+        if (popc(R) + popc(need) > NR) continue;
+        R |= need;
+        sg.push_back((int32_t)i);
+        staged[i] = 1;
+      }
+      if (sg.empty() && !first_stage) {  // cannot happen for a valid DAG
+        plan.ok = false;
+        return plan;
+      }
+      remaining -= sg.size();
+      stage_list.emplace_back(R, std::move(sg));
+    }
+    // a last stage that needs low positions gets a trailing empty high stage
+    if (high_edges && (stage_list.back().first & ~high_pos))
+      stage_list.emplace_back(0u, std::vector<int32_t>());
+
+    for (size_t s = 0; s < stage_list.size(); ++s) {
+      uint32_t R = stage_list[s].first;
+      const bool edge = (s == 0) || (s + 1 == stage_list.size());
+      // pad R to NR positions: high positions on the edges, low ones elsewhere
+      if (edge && high_edges) {
+        for (int p = L; p < T && popc(R) < NR; ++p) R |= 1u << p;
+      }
+      for (int p = 0; p < T && popc(R) < NR; ++p) R |= 1u << p;
+      SwStage st;
+      std::memset(&st, 0, sizeof st);
+      st.nr = NR;
+      int reg_of_pos[32];
+      for (int p = 0; p < 32; ++p) reg_of_pos[p] = -1;
+      {
+        int k = 0;
+        for (uint32_t m = R; m; m &= m - 1) {
+          const int p = __builtin_ctz(m);
+          st.R[k] = (int8_t)p;
+          reg_of_pos[p] = k;
+          ++k;
+        }
+      }
+      st.g0 = (int32_t)plan.gates.size();
+      for (int32_t li : stage_list[s].second) {
+        const PGate& pg = gates[list[li]];
+        SwGate sg;
+        std::memset(&sg, 0, sizeof sg);
+        for (uint64_t m = pg.cmask; m; m &= m - 1) {
+          const int c = __builtin_ctzll(m);
+          if (pos_of[c] >= 0) sg.lmask |= 1u << pos_of[c];
+          else sg.gmask |= 1ULL << c;
+        }
+        auto ref = [&](int q) { return pos_of[q] >= 0 ? pos_of[q] : -q - 1; };
+        sg.moff = (int32_t)plan.pool.size();
+        switch (pg.kind) {
+          case PK_DENSE1:
+            sg.kind = SK_G1;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            plan.pool.insert(plan.pool.end(), pg.m, pg.m + 8);
+            break;
+          case PK_DENSE2:
+            sg.kind = SK_G2;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            sg.b = reg_of_pos[pos_of[pg.q1]];
+            plan.pool.insert(plan.pool.end(), pg.m, pg.m + 32);
+            break;
+          case PK_X:
+            sg.kind = SK_X;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            break;
+          case PK_SWAP:
+            sg.kind = SK_SWAP;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            sg.b = reg_of_pos[pos_of[pg.q1]];
+            break;
+          case PK_DIAG1:
+            sg.kind = SK_D1;
+            sg.a = ref(pg.q0);
+            plan.pool.insert(plan.pool.end(), pg.m, pg.m + 4);
+            break;
+          case PK_DIAG2:
+            sg.kind = SK_D2;
+            sg.a = ref(pg.q0);
+            sg.b = ref(pg.q1);
+            plan.pool.insert(plan.pool.end(), pg.m, pg.m + 8);
+            break;
+        }
+        plan.gates.push_back(sg);
+        plan.gate_ops.push_back(pg.op_index);
+      }
+      st.g1 = (int32_t)plan.gates.size();
+      plan.stages.push_back(st);
+    }
+    sw.s1 = (int32_t)plan.stages.size();
+    plan.sweeps.push_back(sw);
+
+    for (int32_t g : list) idx_in_sweep[g] = -1;
+    ++sweep_id;
+    while (first < G && when[first] >= 0) ++first;
+  }
+  return plan;
+}
+
+}  // namespace sc

@@ -1,0 +1,161 @@
+// Adjoint differentiation entry points (addition; the reference engine has no
+// gradient API).  Two device state buffers (psi, lambda), no stored intermediate
+// states: the reverse pass un-applies each gate from both.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "sc_adjoint.h"
+#include "sc_ctx.h"
+
+namespace sc {
+
+namespace {
+
+void conj_transpose(const double* m, int dim, double* out) {
+  for (int r = 0; r < dim; ++r)
+    for (int c = 0; c < dim; ++c) {
+      out[2 * (dim * c + r)] = m[2 * (dim * r + c)];
+      out[2 * (dim * c + r) + 1] = -m[2 * (dim * r + c) + 1];
+    }
+}
+
+PGate invert(const PGate& g) {
+  PGate h = g;
+  switch (g.kind) {
+    case PK_DENSE1: conj_transpose(g.m, 2, h.m); break;
+    case PK_DENSE2: conj_transpose(g.m, 4, h.m); break;
+    case PK_DIAG1:
+      for (int k = 1; k < 4; k += 2) h.m[k] = -g.m[k];
+      break;
+    case PK_DIAG2:
+      for (int k = 1; k < 8; k += 2) h.m[k] = -g.m[k];
+      break;
+    default: break;  // X and SWAP are self-inverse
+  }
+  return h;
+}
+
+bool generator(const sc_op& op, uint64_t* x, uint64_t* z) {
+  switch (op.kind) {
+    case SC_OP_RX: *x = 1ULL << op.q0; *z = 0; return true;
+    case SC_OP_RY: *x = 1ULL << op.q0; *z = 1ULL << op.q0; return true;  // Y = i X Z
+    case SC_OP_RZ: *x = 0; *z = 1ULL << op.q0; return true;
+    case SC_OP_RZZ: *x = 0; *z = (1ULL << op.q0) | (1ULL << op.q1); return true;
+    default: return false;
+  }
+}
+
+}  // namespace
+
+}  // namespace sc
+
+using namespace sc;
+
+extern "C" {
+
+int32_t sc_adjoint_forward(void* p, int32_t n_qubits, const sc_op* ops, int64_t n_ops,
+                           const double* params, int64_t n_params, int32_t n_terms,
+                           const uint64_t* xmask, const uint64_t* zmask, const double* coeffs,
+                           double* out_value) {
+  Ctx* c = static_cast<Ctx*>(p);
+  if (!c || c->magic != Ctx::kMagic) return fail(SC_EINVAL, "invalid context handle");
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(SC_ECUDA, "cudaSetDevice failed");
+  c->adj_ready = false;
+  if (!c->noise.empty())
+    return fail(SC_EUNSUPPORTED, "adjoint differentiation requires a noiseless circuit");
+  if (n_params < 0 || (n_params > 0 && !params)) return fail(SC_EINVAL, "invalid parameter vector");
+  if (n_terms < 0 || (n_terms > 0 && (!xmask || !zmask || !coeffs)))
+    return fail(SC_EINVAL, "invalid Hamiltonian arrays");
+  for (int64_t i = 0; i < n_ops && ops; ++i) {
+    const int k = ops[i].kind;
+    if ((k == SC_OP_RX || k == SC_OP_RY || k == SC_OP_RZ || k == SC_OP_RZZ) && ops[i].param >= n_params)
+      return fail(SC_EINVAL, "op %lld references parameter %d of %lld", (long long)i, ops[i].param,
+                  (long long)n_params);
+  }
+  int rc = c->run(n_qubits, ops, n_ops, nullptr, 0, false, params, n_params);
+  if (rc != SC_OK) return rc;
+  std::vector<double> terms;
+  if ((rc = c->pauli_terms(n_terms, xmask, zmask, terms)) != SC_OK) return rc;
+  double e = 0.0;
+  for (int32_t t = 0; t < n_terms; ++t) e += coeffs[t] * terms[t];
+  if (out_value) *out_value = e;
+  c->adj_ops.assign(ops, ops + n_ops);
+  c->adj_params.assign(params, params + n_params);
+  c->adj_x.assign(xmask, xmask + n_terms);
+  c->adj_z.assign(zmask, zmask + n_terms);
+  c->adj_c.assign(coeffs, coeffs + n_terms);
+  c->adj_ready = true;
+  return SC_OK;
+}
+
+int32_t sc_adjoint_backward(void* p, double* out_grad, int64_t n_params) {
+  Ctx* c = static_cast<Ctx*>(p);
+  if (!c || c->magic != Ctx::kMagic) return fail(SC_EINVAL, "invalid context handle");
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(SC_ECUDA, "cudaSetDevice failed");
+  if (!c->adj_ready || !c->state_valid)
+    return fail(SC_ESTATE, "sc_adjoint_backward needs a preceding sc_adjoint_forward");
+  if (n_params != (int64_t)c->adj_params.size() || (n_params > 0 && !out_grad))
+    return fail(SC_EINVAL, "gradient buffer must hold %zu entries", c->adj_params.size());
+  const int n = c->n;
+  const size_t amp = (c->cfg.dtype == SC_C64) ? 8 : 16;
+  const int blocks = adjoint_partial_blocks(n, c->sm_count);
+  int rc = c->reserve(c->buf_adj_lambda, amp << n, "adjoint lambda");
+  if (rc != SC_OK) return rc;
+  const size_t scratch = sizeof(double2) * (size_t)blocks + sizeof(double) * (size_t)(n_params + 1);
+  if ((rc = c->reserve(c->buf_adj_phi, scratch, "adjoint scratch")) != SC_OK) return rc;
+  double2* partial = static_cast<double2*>(c->buf_adj_phi.p);
+  double* grad = reinterpret_cast<double*>(partial + blocks);
+  cudaStream_t s = c->stream;
+  void* psi = c->state.p;
+  void* lam = c->buf_adj_lambda.p;
+  const double dim = std::ldexp(1.0, n);
+  cudaError_t e = cudaMemsetAsync(grad, 0, sizeof(double) * (size_t)(n_params + 1), s);
+  if (e != cudaSuccess) return fail_cuda(e, "gradient init");
+
+  // lambda = H psi
+  c->mark_begin(KC_ADJOINT, 3.0 * dim * amp * (double)c->adj_c.size(), (int)c->adj_c.size());
+  if (c->adj_c.empty()) {
+    e = cudaMemsetAsync(lam, 0, amp << n, s);
+  } else {
+    for (size_t t = 0; t < c->adj_c.size() && e == cudaSuccess; ++t)
+      e = launch_pauli_accumulate(c->cfg.dtype, psi, lam, n, c->adj_x[t], c->adj_z[t], c->adj_c[t],
+                                  t > 0, c->sm_count, s);
+  }
+  c->mark_end();
+  if (e != cudaSuccess) return fail_cuda(e, "adjoint H psi");
+
+  for (int64_t i = (int64_t)c->adj_ops.size() - 1; i >= 0; --i) {
+    const sc_op& op = c->adj_ops[i];
+    if (op.kind == SC_OP_MEASURE) continue;
+    PGate g;
+    bool produced = false;
+    normalise_op(op, c->adj_params.data(), (int64_t)c->adj_params.size(), &g, &produced);
+    if (!produced) continue;
+    uint64_t x = 0, z = 0;
+    if (op.param >= 0 && generator(op, &x, &z)) {
+      c->mark_begin(KC_ADJOINT, 2.0 * dim * amp, 2);
+      e = launch_generator_grad(c->cfg.dtype, lam, psi, n, x, z, partial, grad, op.param,
+                                c->sm_count, s);
+      c->mark_end();
+      if (e != cudaSuccess) return fail_cuda(e, "adjoint inner product");
+    }
+    const PGate inv = invert(g);
+    c->mark_begin(KC_ADJOINT, 4.0 * dim * amp, 2);
+    e = launch_gate(c->cfg.dtype, psi, n, inv, s);
+    if (e == cudaSuccess) e = launch_gate(c->cfg.dtype, lam, n, inv, s);
+    c->mark_end();
+    if (e != cudaSuccess) return fail_cuda(e, "adjoint un-apply");
+  }
+  if (n_params > 0 &&
+      (e = cudaMemcpyAsync(out_grad, grad, sizeof(double) * (size_t)n_params,
+                           cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return fail_cuda(e, "gradient download");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return fail_cuda(e, "sc_adjoint_backward");
+  c->collect_timing();
+  c->adj_ready = false;
+  c->state_valid = false;  // psi has been rewound to the initial state
+  return SC_OK;
+}
+
+}  // extern "C"

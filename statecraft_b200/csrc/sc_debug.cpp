@@ -1,0 +1,193 @@
+// Host-side inspection of the fusion planner, usable without a GPU.
+//
+// sc_debug_plan_order reports the order in which the fused kernels apply the
+// ops; sc_debug_emulate_sweeps executes a plan on a host complex128 state with
+// the same tile / stage / register-bit semantics as k_sweep (the shared-memory
+// exchange is a permutation, so a stage is emulated by gathering each thread's
+// 2^NR amplitudes straight from the state).  Tests use both to check the planner
+// and the plan encoding on CPU.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "sc_ctx.h"
+
+using namespace sc;
+
+namespace {
+
+PlanParams debug_params(int tile, int low, int nr, double budget) {
+  PlanParams pp;
+  pp.tile_qubits = tile > 0 ? tile : 11;
+  pp.low_qubits = low > 0 ? low : 4;
+  pp.nr = nr > 0 ? nr : 3;
+  pp.budget = budget;
+  pp.max_gates = 4096;
+  return pp;
+}
+
+int normalise_all(int n, const sc_op* ops, int64_t n_ops, std::vector<PGate>& out) {
+  if (n <= 0 || n > 30) return fail(SC_EINVAL, "debug planner supports 1..30 qubits");
+  for (int64_t i = 0; i < n_ops; ++i) {
+    PGate g;
+    bool produced = false;
+    if (!normalise_op(ops[i], nullptr, 0, &g, &produced))
+      return fail(SC_EINVAL, "op %lld: unknown kind", (long long)i);
+    if (produced) {
+      g.op_index = i;
+      out.push_back(g);
+    }
+  }
+  return SC_OK;
+}
+
+inline uint64_t spread_h(uint32_t x, const SwSweep& sw) {
+  uint64_t g = x & ((1u << sw.L) - 1u);
+  uint32_t hi = x >> sw.L;
+  for (int k = 0; hi; ++k, hi >>= 1)
+    if (hi & 1u) g |= 1ULL << sw.hq[k];
+  return g;
+}
+
+inline int bitref_h(int ref, uint32_t li, uint64_t base) {
+  return ref >= 0 ? (int)((li >> ref) & 1u) : (int)((base >> (-ref - 1)) & 1ULL);
+}
+
+struct C {
+  double r, i;
+};
+inline C cm(double br, double bi, C a) { return {br * a.r - bi * a.i, br * a.i + bi * a.r}; }
+inline C mac2(const double* m0, C a0, const double* m1, C a1) {
+  return {m0[0] * a0.r - m0[1] * a0.i + m1[0] * a1.r - m1[1] * a1.i,
+          m0[0] * a0.i + m0[1] * a0.r + m1[0] * a1.i + m1[1] * a1.r};
+}
+
+void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
+  const int NR = sw.nr, NV = 1 << NR;
+  const uint32_t threads = 1u << (sw.T - NR);
+  std::vector<C> v(NV);
+  std::vector<uint32_t> off(NV);
+  std::vector<uint64_t> gidx(NV);
+  for (int64_t t = 0; t < sw.tiles; ++t) {
+    uint64_t base = (uint64_t)t << sw.L;
+    for (int k = 0; k < sw.h; ++k) {
+      const int b = sw.hq[k];
+      base = ((base >> b) << (b + 1)) | (base & ((1ULL << b) - 1ULL));
+    }
+    for (int s = sw.s0; s < sw.s1; ++s) {
+      const SwStage& stg = plan.stages[s];
+      for (uint32_t tid = 0; tid < threads; ++tid) {
+        uint32_t l0 = tid;
+        for (int k = 0; k < NR; ++k) {
+          const int b = stg.R[k];
+          l0 = ((l0 >> b) << (b + 1)) | (l0 & ((1u << b) - 1u));
+        }
+        for (int j = 0; j < NV; ++j) {
+          uint32_t o = 0;
+          for (int k = 0; k < NR; ++k)
+            if (j & (1 << k)) o |= 1u << stg.R[k];
+          off[j] = o;
+          gidx[j] = base | spread_h(l0 | o, sw);
+          v[j] = {st[2 * gidx[j]], st[2 * gidx[j] + 1]};
+        }
+        for (int gi = stg.g0; gi < stg.g1; ++gi) {
+          const SwGate& g = plan.gates[gi];
+          if ((base & g.gmask) != g.gmask) continue;
+          const double* m = plan.pool.data() + g.moff;
+          auto ok = [&](int j) { return ((l0 | off[j]) & g.lmask) == g.lmask; };
+          switch (g.kind) {
+            case SK_G1:
+            case SK_X:
+              for (int j = 0; j < NV; ++j) {
+                if (j & (1 << g.a)) continue;
+                if (!ok(j)) continue;
+                const int j1 = j | (1 << g.a);
+                if (g.kind == SK_X) {
+                  std::swap(v[j], v[j1]);
+                } else {
+                  const C a0 = v[j], a1 = v[j1];
+                  v[j] = mac2(m + 0, a0, m + 2, a1);
+                  v[j1] = mac2(m + 4, a0, m + 6, a1);
+                }
+              }
+              break;
+            case SK_G2:
+              for (int j = 0; j < NV; ++j) {
+                if (j & ((1 << g.a) | (1 << g.b))) continue;
+                const int idx[4] = {j, j | (1 << g.b), j | (1 << g.a), j | (1 << g.a) | (1 << g.b)};
+                C a[4], o[4];
+                for (int k = 0; k < 4; ++k) a[k] = v[idx[k]];
+                for (int r = 0; r < 4; ++r) {
+                  o[r] = {0.0, 0.0};
+                  for (int c = 0; c < 4; ++c) {
+                    const double mr = m[2 * (4 * r + c)], mi = m[2 * (4 * r + c) + 1];
+                    o[r].r += mr * a[c].r - mi * a[c].i;
+                    o[r].i += mr * a[c].i + mi * a[c].r;
+                  }
+                }
+                for (int k = 0; k < 4; ++k) v[idx[k]] = o[k];
+              }
+              break;
+            case SK_SWAP:
+              for (int j = 0; j < NV; ++j) {
+                if (j & ((1 << g.a) | (1 << g.b))) continue;
+                std::swap(v[j | (1 << g.a)], v[j | (1 << g.b)]);
+              }
+              break;
+            case SK_D1:
+              for (int j = 0; j < NV; ++j) {
+                if (!ok(j)) continue;
+                const int bit = bitref_h(g.a, l0 | off[j], base);
+                v[j] = cm(m[2 * bit], m[2 * bit + 1], v[j]);
+              }
+              break;
+            case SK_D2:
+              for (int j = 0; j < NV; ++j) {
+                const uint32_t li = l0 | off[j];
+                const int k = (bitref_h(g.a, li, base) << 1) | bitref_h(g.b, li, base);
+                v[j] = cm(m[2 * k], m[2 * k + 1], v[j]);
+              }
+              break;
+          }
+        }
+        for (int j = 0; j < NV; ++j) {
+          st[2 * gidx[j]] = v[j].r;
+          st[2 * gidx[j] + 1] = v[j].i;
+        }
+      }
+    }
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                            int32_t low_qubits, int32_t nr, double budget, int64_t* order,
+                            int64_t* n_sweeps, int64_t* n_stages) {
+  std::vector<PGate> gates;
+  int rc = normalise_all(n, ops, n_ops, gates);
+  if (rc != SC_OK) return rc;
+  Plan plan = plan_sweeps(gates, n, debug_params(tile_qubits, low_qubits, nr, budget));
+  if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+  if (order)
+    for (size_t i = 0; i < plan.gate_ops.size(); ++i) order[i] = plan.gate_ops[i];
+  if (n_sweeps) *n_sweeps = (int64_t)plan.sweeps.size();
+  if (n_stages) *n_stages = (int64_t)plan.stages.size();
+  return (int32_t)plan.gate_ops.size();
+}
+
+int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                                int32_t low_qubits, int32_t nr, double budget, double* state) {
+  std::vector<PGate> gates;
+  int rc = normalise_all(n, ops, n_ops, gates);
+  if (rc != SC_OK) return rc;
+  if (!state) return fail(SC_EINVAL, "state is null");
+  Plan plan = plan_sweeps(gates, n, debug_params(tile_qubits, low_qubits, nr, budget));
+  if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+  for (const SwSweep& sw : plan.sweeps) emulate_sweep(state, plan, sw);
+  return (int32_t)plan.sweeps.size();
+}
+
+}  // extern "C"

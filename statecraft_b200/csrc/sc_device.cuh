@@ -1,0 +1,80 @@
+// Device helpers shared by the kernels: amplitude types, complex arithmetic,
+// index bit manipulation and the shared-memory swizzle.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sc {
+
+// Amplitude storage: complex128 = double2 (16 B), complex64 = float2 (8 B).
+template <typename R> struct Amp;
+template <> struct Amp<double> {
+  using type = double2;
+  // 128-byte shared-memory row = 8 amplitudes
+  static constexpr int kSwizzleShift = 3;
+};
+template <> struct Amp<float> {
+  using type = float2;
+  static constexpr int kSwizzleShift = 4;
+};
+
+template <typename R>
+__device__ __forceinline__ typename Amp<R>::type make_amp(R re, R im) {
+  typename Amp<R>::type a;
+  a.x = re;
+  a.y = im;
+  return a;
+}
+
+// (ar + i ai) * (br + i bi)
+template <typename A, typename R>
+__device__ __forceinline__ A cmul(R br, R bi, A a) {
+  A o;
+  o.x = br * a.x - bi * a.y;
+  o.y = br * a.y + bi * a.x;
+  return o;
+}
+
+// m0 * a0 + m1 * a1 with m given as (re, im) pairs
+template <typename A, typename R>
+__device__ __forceinline__ A cmac2(R m0r, R m0i, A a0, R m1r, R m1i, A a1) {
+  A o;
+  o.x = m0r * a0.x - m0i * a0.y + m1r * a1.x - m1i * a1.y;
+  o.y = m0r * a0.y + m0i * a0.x + m1r * a1.y + m1i * a1.x;
+  return o;
+}
+
+__host__ __device__ __forceinline__ uint64_t insert_zero64(uint64_t x, int bit) {
+  const uint64_t low = x & ((1ULL << bit) - 1ULL);
+  return ((x >> bit) << (bit + 1)) | low;
+}
+
+__host__ __device__ __forceinline__ uint32_t insert_zero32(uint32_t x, int bit) {
+  const uint32_t low = x & ((1u << bit) - 1u);
+  return ((x >> bit) << (bit + 1)) | low;
+}
+
+// XOR swizzle of shared-memory slots: the 16-byte chunk index inside each
+// 128-byte row is XORed with the row index (mod chunks per row).  Stage gathers
+// whose lanes stride by whole rows then hit distinct banks.
+template <typename R>
+__device__ __forceinline__ uint32_t swz(uint32_t i) {
+  constexpr int s = Amp<R>::kSwizzleShift;
+  return i ^ ((i >> s) & ((1u << s) - 1u));
+}
+
+// SplitMix64 (java.util.SplittableRandom): the k-th nextDouble() (k = 0, 1, ...)
+// of a generator seeded with `seed` is a pure function of (seed, k).
+__host__ __device__ __forceinline__ uint64_t splitmix_mix64(uint64_t z) {
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+constexpr uint64_t kGoldenGamma = 0x9e3779b97f4a7c15ULL;
+__host__ __device__ __forceinline__ double splitmix_double(uint64_t seed, uint64_t k) {
+  const uint64_t z = splitmix_mix64(seed + (k + 1ULL) * kGoldenGamma);
+  return (double)(z >> 11) * 0x1.0p-53;
+}
+
+}  // namespace sc

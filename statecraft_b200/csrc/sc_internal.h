@@ -1,0 +1,145 @@
+// Internal declarations shared by the C ABI, the fusion planner and the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/statecraft_b200.h"
+
+namespace sc {
+
+// ---------------------------------------------------------------------------
+// normalised gates (host)
+// ---------------------------------------------------------------------------
+// Every unitary sc_op is normalised into one of these before planning:
+//   PK_DENSE1  2x2 on q0 (optionally controlled by cmask)      m[0..7]
+//   PK_DENSE2  4x4 on (q0 = first, q1 = second)                m[0..31]
+//   PK_X       controlled pair swap on target q0 (CNOT / MCX)   -
+//   PK_SWAP    swap of qubits q0, q1                            -
+//   PK_DIAG1   diag(d0, d1) on q0, optionally controlled        m[0..3]
+//   PK_DIAG2   diag(d[4]) on (q0 = first, q1 = second)          m[0..7]
+enum PKind : int32_t { PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2 };
+
+struct PGate {
+  int32_t kind;
+  int32_t q0, q1;
+  uint64_t cmask;
+  double m[32];
+  int64_t op_index;
+};
+
+// FMA-per-amplitude cost model used by the planner.
+double gate_cost(const PGate& g);
+uint64_t dense_mask(const PGate& g);
+uint64_t touch_mask(const PGate& g);
+
+// Converts one validated sc_op into zero or one PGate (MEASURE -> none).
+// params/n_params resolve SC_OP_R* angles.  Returns false for unknown kinds.
+bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate* out,
+                  bool* produced);
+
+// ---------------------------------------------------------------------------
+// fused tile sweeps (device-visible plan records)
+// ---------------------------------------------------------------------------
+// A sweep moves every amplitude through a CTA once.  A tile holds the 2^T
+// amplitudes whose indices differ only in the tile qubits: the L lowest qubits
+// (tile positions 0..L-1) plus h = T - L "high" qubits hq[] (positions L..T-1).
+// Inside the tile, a stage gives each thread 2^NR amplitudes that differ in the
+// NR tile positions R[0..NR-1] (ascending); every gate of the stage acts on those
+// register bits (dense / permutation kinds) or on any bit (diagonal kinds).
+enum SwKind : int32_t { SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2 };
+
+constexpr int SW_MAX_HIGH = 24;
+constexpr int SW_MAX_NR = 4;
+
+struct SwGate {     // 32 bytes
+  int32_t kind;     // SwKind
+  int32_t a, b;     // register bits (G1/G2/X/SWAP) or diagonal qubit refs (D1/D2):
+                    //   ref >= 0 -> tile position, ref < 0 -> global qubit (-ref - 1)
+  int32_t moff;     // offset of the matrix in the sweep pool (reals)
+  uint32_t lmask;   // control bits on tile positions
+  uint32_t pad;
+  uint64_t gmask;   // control bits on global (non-tile) qubits
+};
+
+struct SwStage {    // 16 bytes
+  int32_t g0, g1;   // gate range
+  int8_t R[SW_MAX_NR];
+  int32_t nr;       // number of meaningful register positions (== kernel NR)
+};
+
+struct SwSweep {
+  int32_t T, L, h, nr;
+  int32_t s0, s1;            // stage range
+  int64_t tiles;
+  int32_t hq[SW_MAX_HIGH];   // ascending
+};
+
+struct PlanParams {
+  int tile_qubits;   // T (clamped to n)
+  int low_qubits;    // L
+  int nr;            // register qubits per stage
+  double budget;     // FMA per amplitude per sweep; < 0 unlimited
+  int max_gates;     // per sweep
+};
+
+struct Plan {
+  std::vector<SwSweep> sweeps;
+  std::vector<SwStage> stages;
+  std::vector<SwGate> gates;
+  std::vector<double> pool;
+  std::vector<int64_t> gate_ops;  // host only: op index of each entry of `gates`
+  int64_t n_gates = 0;
+  bool ok = true;  // false if some gate could not be staged (planner invariant broken)
+};
+
+// Builds the sweep plan for a gate list on n qubits.
+Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp);
+
+
+// ---------------------------------------------------------------------------
+// kernel classes (timing / statistics)
+// ---------------------------------------------------------------------------
+enum KernelClass : int32_t {
+  KC_SWEEP = 0,
+  KC_GATE_DENSE,
+  KC_GATE_PERM,
+  KC_GATE_DIAG,
+  KC_INIT,
+  KC_PROB,
+  KC_SAMPLE,
+  KC_NOISE,
+  KC_EXPECT,
+  KC_ADJOINT,
+  KC_BATCH,
+  KC_COUNT
+};
+const char* kernel_class_name(int cls);
+
+// ---------------------------------------------------------------------------
+// launchers (implemented in the .cu files; all asynchronous on `stream`)
+// ---------------------------------------------------------------------------
+struct DevPlan {
+  SwStage* stages = nullptr;
+  SwGate* gates = nullptr;
+  void* pool = nullptr;   // double (c128) or float (c64)
+  size_t cap_stages = 0, cap_gates = 0, cap_pool = 0;
+};
+
+// per-gate path (fusion off); `state` is double2* or float2* per dtype
+cudaError_t launch_gate(int dtype, void* state, int n, const PGate& g, cudaStream_t s);
+// fused sweep
+cudaError_t launch_sweep(int dtype, void* state, int n, const SwSweep& sw, const DevPlan& dp,
+                         int sm_count, cudaStream_t s);
+// |0..0> or |basis>
+cudaError_t launch_init_basis(int dtype, void* state, int n, uint64_t basis, cudaStream_t s);
+// c128 host layout -> device amplitudes (dtype conversion for c64)
+cudaError_t launch_convert_in(int dtype, void* state, const double* src, int64_t count,
+                              cudaStream_t s);
+cudaError_t launch_convert_out(int dtype, const void* state, double* dst, int64_t count,
+                               cudaStream_t s);
+
+}  // namespace sc

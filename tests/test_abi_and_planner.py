@@ -1,0 +1,142 @@
+"""CPU tests of the native library: symbol exports, ABI layout, failure without a
+GPU, and the fusion planner (order respects the dependency DAG; the plan encoding,
+executed with the kernel's tile/stage semantics on the host, matches the oracle)."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import randcirc as RCirc
+from oracle import oracle as O
+from statecraft_b200 import _abi as A
+from statecraft_b200.engine import serialize_circuit
+
+HEADER = Path(__file__).resolve().parents[1] / "include" / "statecraft_b200.h"
+
+
+def declared_symbols():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^SC_API\s+[\w\s\*]+?\b(sc_\w+)\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = A.load()
+    syms = declared_symbols()
+    assert len(syms) >= 19
+    for name in syms:
+        assert hasattr(lib, name), name
+    assert set(syms) == set(A.SIGNATURES), "ctypes signature table out of sync with the header"
+
+
+def test_abi_version_and_struct_sizes():
+    lib = A.load()
+    assert lib.sc_version() == A.SC_ABI_VERSION
+    assert ctypes.sizeof(A.ScOp) == 280
+    assert ctypes.sizeof(A.ScChannel) == 528
+    assert ctypes.sizeof(A.ScConfig) == 32
+
+
+def test_create_without_gpu_fails_cleanly():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    lib = A.load()
+    h = ctypes.c_void_p()
+    rc = lib.sc_create(0, None, ctypes.byref(h))
+    assert rc in (A.SC_ECUDA, A.SC_EINVAL)
+    assert lib.sc_last_error()
+    assert not h.value
+
+
+def test_invalid_handle_rejected():
+    lib = A.load()
+    assert lib.sc_destroy(None) == A.SC_OK
+
+
+def _plan_order(c, tile, low, nr, budget):
+    ops, n_ops = serialize_circuit(c)
+    order = np.zeros(max(1, n_ops), dtype=np.int64)
+    sweeps = ctypes.c_int64()
+    stages = ctypes.c_int64()
+    k = A.load().sc_debug_plan_order(c.qubitCount, ops, n_ops, tile, low, nr, budget,
+                                     order.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                     ctypes.byref(sweeps), ctypes.byref(stages))
+    assert k >= 0
+    return order[:k], sweeps.value, stages.value
+
+
+def _emulate(c, state, tile, low, nr, budget):
+    ops, n_ops = serialize_circuit(c)
+    st = state.copy()
+    rc = A.load().sc_debug_emulate_sweeps(c.qubitCount, ops, n_ops, tile, low, nr, budget,
+                                          st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert rc >= 0, A.load().sc_last_error()
+    return st, rc
+
+
+def _oracle(c, state):
+    ops, n_ops = serialize_circuit(c)
+    st = state.copy()
+    rc, _ = O.run(c.qubitCount, ops, n_ops, st)
+    assert rc == 0
+    return st
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 5, 8, 11, 13])
+@pytest.mark.parametrize("cfg", [(11, 4, 3, 96.0), (6, 2, 2, -1.0), (9, 5, 4, 24.0), (12, 3, 1, 8.0)])
+def test_emulated_plan_matches_oracle(n, cfg):
+    tile, low, nr, budget = cfg
+    for seed in range(3):
+        c = RCirc.random_circuit(n, 40, seed=1000 * n + seed)
+        init = RCirc.random_state(n, seed)
+        got, sweeps = _emulate(c, init, tile, low, nr, budget)
+        want = _oracle(c, init)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+
+
+def test_plan_order_is_a_permutation_and_respects_dependencies():
+    c = RCirc.random_circuit(12, 300, seed=7)
+    order, sweeps, stages = _plan_order(c, 11, 4, 3, 96.0)
+    ops = c.operations
+    assert sorted(order.tolist()) == list(range(len(ops)))
+    # two ops keep their relative order when a qubit is touched by both and acted
+    # on non-diagonally (as a target of a non-diagonal gate) by at least one
+    pos = {int(o): k for k, o in enumerate(order)}
+    for i in range(len(ops)):
+        for j in range(i + 1, len(ops)):
+            shared = (set(ops[i].qubits_touched()) & set(ops[j].qubits_touched()))
+            if shared & (_dense_qubits(ops[i]) | _dense_qubits(ops[j])):
+                assert pos[i] < pos[j], (i, j, ops[i], ops[j])
+
+
+def _is_diag(gate) -> bool:
+    return gate.element(0, 1) == 0 and gate.element(1, 0) == 0
+
+
+def _dense_qubits(op) -> set:
+    from statecraft_b200 import quantum as Q
+
+    if isinstance(op, Q.SingleGateOperation):
+        return set() if _is_diag(op.gate) else {op.qubit}
+    if isinstance(op, Q.CnotOperation):
+        return {op.targetQubit}
+    if isinstance(op, Q.TwoQubitGateOperation):
+        m = np.array(op.matrix).reshape(4, 4)
+        return set() if np.count_nonzero(m - np.diag(np.diag(m))) == 0 else {op.firstQubit, op.secondQubit}
+    if isinstance(op, Q.SwapOperation):
+        return {op.firstQubit, op.secondQubit}
+    if isinstance(op, Q.MultiControlOperation):
+        return set() if _is_diag(op.gate) else {op.targetQubit}
+    return set()
+
+
+def test_brickwall_plan_uses_few_sweeps():
+    from statecraft_b200 import workloads as W
+
+    c = W.brickwall_circuit(20, 20, seed=2020, mcz=False, rzz=False)
+    order, sweeps, stages = _plan_order(c, 11, 4, 3, -1.0)
+    assert len(order) == len(c.operations)
+    assert sweeps <= 3 * 20  # unfused would be 590 sweeps
