@@ -102,7 +102,7 @@ typedef struct sc_config {
                                Exceeding it returns SC_ENOMEM without calling the allocator. */
 } sc_config;
 
-#define SC_DEFAULT_MAX_QUBITS 33
+#define SC_DEFAULT_MAX_QUBITS 32
 
 /* ---- library / context --------------------------------------------------- */
 SC_API int32_t sc_version(void);

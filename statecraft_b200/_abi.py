@@ -36,7 +36,7 @@ SC_OP_RZ = 18
 SC_OP_RZZ = 19
 
 SC_MAX_KRAUS = 8
-SC_DEFAULT_MAX_QUBITS = 33
+SC_DEFAULT_MAX_QUBITS = 32
 
 
 class ScOp(ctypes.Structure):

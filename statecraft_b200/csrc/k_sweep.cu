@@ -2,37 +2,37 @@
 // applies every gate the planner packed into the sweep.
 //
 // Tile: the 2^T amplitudes whose indices differ only in the tile qubits (the L
-// lowest qubits, contiguous in memory, plus h high qubits).  A persistent CTA
-// walks tiles.  Per tile it runs the sweep's stages; in stage s each thread holds
-// 2^NR amplitudes in registers that differ in the stage's register positions
-// R[0..NR-1], applies the stage's gates there, and the next stage re-distributes
-// the tile through XOR-swizzled shared memory.  The first stage loads straight
-// from HBM and the last stage stores straight to HBM: with R on high positions,
-// the lanes of a warp walk the low (contiguous) positions, so every warp access is
-// a contiguous 2^min(L,5)-amplitude run of 128-bit (c128) / 64-bit (c64) words.
+// lowest qubits, contiguous in memory, plus h high qubits), i.e. 2^h contiguous
+// segments of 2^L amplitudes.  A persistent CTA walks tiles with two shared-memory
+// tile buffers: while it computes tile i in one buffer, TMA bulk copies
+// (cp.async.bulk, one per segment, completing on an mbarrier) stream tile i+1 into
+// the other, and the results of tile i drain to HBM as bulk stores.
+//
+// Per tile the sweep's stages run in registers: in stage s each thread holds 2^NR
+// amplitudes that differ in the stage's register positions R[0..NR-1] and applies
+// the stage's gates there; the next stage re-distributes the tile through the
+// buffer with an XOR swizzle.  The first stage reads and the last stage writes the
+// buffer in the linear (TMA) layout; with R on high positions the lanes of a warp
+// walk the low positions, so those accesses are conflict-free too.
+//
+// The whole sweep plan (stages, register tables, gates, matrices) is a
+// __grid_constant__ kernel parameter: every thread reads the same record at the
+// same time, which the constant cache serves as a broadcast.
+//
+// Every mbarrier wait is bounded (about a second of clock cycles); on timeout the
+// CTA records an error in `err`, waits (bounded) for the copies it issued and
+// returns, and the host reports SC_ETIMEOUT.
 #include <algorithm>
 #include <mutex>
 #include <type_traits>
 
 #include "sc_device.cuh"
 #include "sc_internal.h"
+#include "sc_sweep.h"
 
 namespace sc {
 
 namespace {
-
-// local tile index -> global index bits (without the tile base)
-__device__ __forceinline__ uint64_t spread(uint32_t x, const SwSweep& sw) {
-  uint64_t g = x & ((1u << sw.L) - 1u);
-  uint32_t hi = x >> sw.L;
-  for (int k = 0; hi; ++k, hi >>= 1)
-    if (hi & 1u) g |= 1ULL << sw.hq[k];
-  return g;
-}
-
-__device__ __forceinline__ int bit_ref(int ref, uint32_t lidx, uint64_t base) {
-  return ref >= 0 ? (int)((lidx >> ref) & 1u) : (int)((base >> (-ref - 1)) & 1ULL);
-}
 
 template <typename R, int NR, int A_>
 __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R* m,
@@ -42,8 +42,7 @@ __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R*
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j) {
     if (j & (1 << A_)) continue;
-    constexpr int bit = 1 << A_;
-    const int j1 = j | bit;
+    const int j1 = j | (1 << A_);
     if (lmask && (((l0 | off[j]) & lmask) != lmask)) continue;
     const auto a0 = v[j], a1 = v[j1];
     v[j] = cmac2(m00r, m00i, a0, m01r, m01i, a1);
@@ -58,10 +57,10 @@ __device__ __forceinline__ void xswap(typename Amp<R>::type (&v)[1 << NR], uint3
   for (int j = 0; j < (1 << NR); ++j) {
     if (j & (1 << A_)) continue;
     const int j1 = j | (1 << A_);
-    if (lmask && (((l0 | off[j]) & lmask) != lmask)) continue;
-    const auto t = v[j];
-    v[j] = v[j1];
-    v[j1] = t;
+    const bool on = ((l0 | off[j]) & lmask) == lmask;
+    const auto a0 = v[j], a1 = v[j1];
+    v[j] = on ? a1 : a0;
+    v[j1] = on ? a0 : a1;
   }
 }
 
@@ -124,70 +123,182 @@ __device__ __forceinline__ void dispatch2(int a, int b, F&& f) {
   });
 }
 
-// Block size is 2^(T - NR); the bound keeps >= 128 registers for NR >= 3.
+// local tile index -> global offset (n <= 32: 32-bit)
+template <typename P>
+__device__ __forceinline__ uint32_t spread32(uint32_t x, const P& p) {
+  uint32_t g = x & ((1u << p.L) - 1u);
+  uint32_t hi = x >> p.L;
+#pragma unroll 1
+  for (int k = 0; hi; ++k, hi >>= 1)
+    if (hi & 1u) g |= 1u << p.hq[k];
+  return g;
+}
+
+// the thread's index bits placed around the stage's register positions
+template <int NR>
+__device__ __forceinline__ uint32_t stage_l0(uint32_t tid, const SwStage& s) {
+  uint32_t x = tid;
+#pragma unroll
+  for (int k = 0; k < NR; ++k) x = insert_zero32(x, s.R[k]);
+  return x;
+}
+
+template <typename P>
+__device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
+  uint32_t base = t << p.L;
+#pragma unroll 1
+  for (int k = 0; k < p.h; ++k) base = insert_zero32(base, p.hq[k]);
+  return base;
+}
+
 template <typename R, int NR>
 constexpr int sweep_max_threads() {
   return NR >= 4 ? (sizeof(R) == 8 ? 256 : 512) : (NR == 3 ? 512 : 1024);
 }
 
-template <typename R, int NR>
+constexpr long long kWaitLimitCycles = 2000000000LL;  // ~1 s at 2 GHz
+
+template <typename R>
+__host__ __device__ constexpr size_t sweep_smem_bytes(int T, int h, bool tma, int stages) {
+  return tma ? 2 * (sizeof(typename Amp<R>::type) << T) + 64 + 4 * ((size_t)1 << h)
+             : (stages > 1 ? (sizeof(typename Amp<R>::type) << T) : 0);
+}
+
+// kTma = true: double-buffered bulk-copy pipeline (worth it for long segments);
+// kTma = false: direct 128-/64-bit loads and stores, one exchange buffer.
+template <typename R, int NR, bool kTma>
 __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
-    k_sweep(typename Amp<R>::type* __restrict__ st, const SwSweep sw,
-            const SwStage* __restrict__ stages, const SwGate* __restrict__ gates,
-            const R* __restrict__ pool) {
+    k_sweep(typename Amp<R>::type* __restrict__ st, const __grid_constant__ SweepParams<R> p,
+            int* __restrict__ err) {
   using A = typename Amp<R>::type;
   constexpr int NV = 1 << NR;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  A* tile = reinterpret_cast<A*>(smem_raw);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const uint32_t tile_amps = 1u << p.T;
+  A* const buf0 = reinterpret_cast<A*>(smem_raw);
+  A* const buf1 = buf0 + tile_amps;
+  uint64_t* const bars = reinterpret_cast<uint64_t*>(buf1 + tile_amps);
+  int* const s_abort = reinterpret_cast<int*>(bars + 2);
+  uint32_t* const segoff = reinterpret_cast<uint32_t*>(bars + 8);
   const uint32_t tid = threadIdx.x;
+  const uint32_t lane = tid & 31u;
+  // warp 0 (all of it, or the whole block when it is smaller) issues every bulk copy
+  const uint32_t nprod = blockDim.x < 32u ? blockDim.x : 32u;
+  const unsigned pmask = nprod == 32u ? 0xffffffffu : ((1u << nprod) - 1u);
+  const bool producer = tid < nprod;
+  const int ns = p.n_stages;
+  const uint32_t nseg = 1u << p.h;
+  const uint32_t seg_amps = 1u << p.L;
+  const uint32_t seg_bytes = seg_amps * (uint32_t)sizeof(A);
+  const uint32_t tile_bytes = tile_amps * (uint32_t)sizeof(A);
+  const uint32_t tiles = (uint32_t)p.tiles;
 
-  for (int64_t t = blockIdx.x; t < sw.tiles; t += gridDim.x) {
-    uint64_t base = (uint64_t)t << sw.L;
-    for (int k = 0; k < sw.h; ++k) base = insert_zero64(base, sw.hq[k]);
+  if constexpr (kTma) {
+    // global offset of each segment (the high tile bits spread onto hq)
+    for (uint32_t sidx = tid; sidx < nseg; sidx += blockDim.x) {
+      uint32_t g = 0;
+      for (int k = 0; k < p.h; ++k)
+        if ((sidx >> k) & 1u) g |= 1u << p.hq[k];
+      segoff[sidx] = g;
+    }
+    if (tid == 0) {
+      mbar_init(&bars[0], 1);
+      mbar_init(&bars[1], 1);
+      *s_abort = 0;
+      mbar_init_fence();
+    }
+    __syncthreads();
+  }
+
+  auto issue_load = [&](uint32_t t, int b) {
+    const A* src = st + tile_base(t, p);
+    A* dst = b ? buf1 : buf0;
+    if (lane == 0) mbar_arrive_expect_tx(&bars[b], tile_bytes);
+    __syncwarp(pmask);
+    for (uint32_t s = lane; s < nseg; s += nprod)
+      bulk_load(dst + s * seg_amps, src + segoff[s], seg_bytes, &bars[b]);
+  };
+
+  // first (load) and last (store) register layouts are tile-invariant
+  const uint32_t l0_first = stage_l0<NR>(tid, p.stages[0]);
+  const uint32_t l0_last = stage_l0<NR>(tid, p.stages[ns - 1]);
+  const uint32_t gt_first = kTma ? 0u : spread32(l0_first, p);
+  const uint32_t gt_last = kTma ? 0u : spread32(l0_last, p);
+
+  uint32_t t = blockIdx.x;
+  uint32_t i = 0;
+  if constexpr (kTma) {
+    if (producer && t < tiles) issue_load(t, 0);
+  }
+  bool aborted = false;
+  for (; t < tiles; t += gridDim.x, ++i) {
+    const int b = kTma ? (int)(i & 1u) : 0;
+    A* const cur = b ? buf1 : buf0;
+    if constexpr (kTma) {
+      const uint32_t tn = t + gridDim.x;
+      if (producer && tn < tiles) {
+        bulk_wait_read_all();  // the other buffer's previous bulk stores have read it
+        fence_proxy_async_smem();
+        issue_load(tn, b ^ 1);
+      }
+      if (!mbar_wait_bounded(&bars[b], (i >> 1) & 1u, kWaitLimitCycles)) {
+        *s_abort = 1;
+        atomicExch(err, 1);
+      }
+      __syncthreads();
+      if (*s_abort) {
+        aborted = true;
+        break;
+      }
+    }
+    const uint32_t base = tile_base(t, p);
 
     A v[NV];
-    uint32_t l0 = 0;
-    uint32_t off[NV];
-    for (int s = sw.s0; s < sw.s1; ++s) {
-      const SwStage stg = stages[s];
-      uint32_t nl0 = tid;
+    if constexpr (kTma) {
+      const SwStageTab& tab = p.tabs[0];
 #pragma unroll
-      for (int k = 0; k < NR; ++k) nl0 = insert_zero32(nl0, stg.R[k]);
-      uint32_t noff[NV];
+      for (int j = 0; j < NV; ++j) v[j] = cur[l0_first | tab.off[j]];
+    } else {
+      const A* __restrict__ src = st + base;
 #pragma unroll
-      for (int j = 0; j < NV; ++j) {
-        uint32_t o = 0;
+      for (int j = 0; j < NV; ++j) v[j] = src[gt_first | p.gfirst[j]];
+    }
+    uint32_t l0 = l0_first, off[NV], sidx[NV];
+#pragma unroll 1
+    for (int s = 0; s < ns; ++s) {
+      const SwStage& stg = p.stages[s];
+      const SwStageTab& tab = p.tabs[s];
+      const uint32_t nl0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
+      const uint32_t sw0 = swz<R>(nl0);
+      if (s > 0) {
+        __syncthreads();  // readers of the buffer are done
 #pragma unroll
-        for (int k = 0; k < NR; ++k)
-          if (j & (1 << k)) o |= 1u << stg.R[k];
-        noff[j] = o;
-      }
-      if (s == sw.s0) {
-        const uint64_t g0 = base | spread(nl0, sw);
-#pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = st[g0 | spread(noff[j], sw)];
-      } else {
-        __syncthreads();  // previous readers of the tile are done
-#pragma unroll
-        for (int j = 0; j < NV; ++j) tile[swz<R>(l0 | off[j])] = v[j];
+        for (int j = 0; j < NV; ++j) cur[sidx[j]] = v[j];
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = tile[swz<R>(nl0 | noff[j])];
+        for (int j = 0; j < NV; ++j) {
+          sidx[j] = sw0 ^ tab.soff[j];
+          v[j] = cur[sidx[j]];
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.soff[j];
       }
       l0 = nl0;
 #pragma unroll
-      for (int j = 0; j < NV; ++j) off[j] = noff[j];
+      for (int j = 0; j < NV; ++j) off[j] = tab.off[j];
 
+#pragma unroll 1
       for (int gi = stg.g0; gi < stg.g1; ++gi) {
-        const SwGate g = gates[gi];
-        if ((base & g.gmask) != g.gmask) continue;
-        const R* m = pool + g.moff;
+        const SwGate& g = p.gates[gi];
+        if (((uint64_t)base & g.gmask) != g.gmask) continue;
+        const R* m = p.pool + g.moff;
+        const uint32_t lmask = g.lmask;
         switch (g.kind) {
           case SK_G1:
-            dispatch1<NR>(g.a, [&](auto ia) { g1<R, NR, decltype(ia)::value>(v, m, l0, off, g.lmask); });
+            dispatch1<NR>(g.a, [&](auto ia) { g1<R, NR, decltype(ia)::value>(v, m, l0, off, lmask); });
             break;
           case SK_X:
-            dispatch1<NR>(g.a, [&](auto ia) { xswap<R, NR, decltype(ia)::value>(v, l0, off, g.lmask); });
+            dispatch1<NR>(g.a, [&](auto ia) { xswap<R, NR, decltype(ia)::value>(v, l0, off, lmask); });
             break;
           case SK_G2:
             if constexpr (NR > 1)
@@ -207,21 +318,46 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
               });
             break;
           case SK_D1: {
+            // diag(d0, d1) on one bit; the bit is a tile position (a >= 0) or a
+            // global qubit fixed for the whole tile (a < 0)
+            const int a = g.a;
+            const uint32_t gb = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
+            const int sh = a < 0 ? 0 : a;
+            const uint32_t lm = a < 0 ? 0u : 1u;
             const R d0r = m[0], d0i = m[1], d1r = m[2], d1i = m[3];
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
               const uint32_t li = l0 | off[j];
-              if ((li & g.lmask) != g.lmask) continue;
-              const int bit = bit_ref(g.a, li, base);
-              v[j] = bit ? cmul(d1r, d1i, v[j]) : cmul(d0r, d0i, v[j]);
+              if ((li & lmask) != lmask) continue;
+              const uint32_t bit = ((li >> sh) & lm) | gb;
+              v[j] = cmul(bit ? d1r : d0r, bit ? d1i : d0i, v[j]);
+            }
+            break;
+          }
+          case SK_DP: {
+            // parity diagonal: factor d[bit(a) ^ bit(b)]
+            const int a = g.a, bq = g.b;
+            const uint32_t gpar = (a < 0 ? ((base >> (-a - 1)) & 1u) : 0u) ^
+                                  (bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u);
+            const uint32_t pm = (a < 0 ? 0u : (1u << a)) | (bq < 0 ? 0u : (1u << bq));
+            const R d0r = m[0], d0i = m[1], d1r = m[2], d1i = m[3];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) {
+              const uint32_t bit = (__popc((l0 | off[j]) & pm) & 1u) ^ gpar;
+              v[j] = cmul(bit ? d1r : d0r, bit ? d1i : d0i, v[j]);
             }
             break;
           }
           case SK_D2: {
+            const int a = g.a, bq = g.b;
+            const uint32_t ga = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
+            const uint32_t gbb = bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u;
+            const int sa = a < 0 ? 0 : a, sb = bq < 0 ? 0 : bq;
+            const uint32_t ma = a < 0 ? 0u : 1u, mb = bq < 0 ? 0u : 1u;
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
               const uint32_t li = l0 | off[j];
-              const int k = (bit_ref(g.a, li, base) << 1) | bit_ref(g.b, li, base);
+              const uint32_t k = ((((li >> sa) & ma) | ga) << 1) | (((li >> sb) & mb) | gbb);
               v[j] = cmul(m[2 * k], m[2 * k + 1], v[j]);
             }
             break;
@@ -230,65 +366,174 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
         }
       }
     }
-    const uint64_t g0 = base | spread(l0, sw);
+    if constexpr (kTma) {
+      // stage the results in the linear layout and drain them with bulk stores
+      __syncthreads();  // every read of `cur` is done
+      {
+        const SwStageTab& tab = p.tabs[ns - 1];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) st[g0 | spread(off[j], sw)] = v[j];
+        for (int j = 0; j < NV; ++j) cur[l0_last | tab.off[j]] = v[j];
+      }
+      fence_proxy_async_smem();
+      __syncthreads();
+      if (producer) {
+        A* dst = st + base;
+        for (uint32_t s = lane; s < nseg; s += nprod)
+          bulk_store(dst + segoff[s], cur + s * seg_amps, seg_bytes);
+        bulk_commit();
+      }
+    } else {
+      A* __restrict__ dst = st + base;
+#pragma unroll
+      for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
+    }
+  }
+  if constexpr (kTma) {
+    if (aborted && producer) {
+      // wait (bounded) for the loads this CTA still has in flight before leaving
+      const uint32_t tn = t + gridDim.x;
+      mbar_wait_bounded(&bars[i & 1u], (i >> 1) & 1u, kWaitLimitCycles);
+      if (tn < tiles) mbar_wait_bounded(&bars[(i + 1) & 1u], ((i + 1) >> 1) & 1u, kWaitLimitCycles);
+    }
+    if (producer) bulk_wait_all();
   }
 }
 
 struct LaunchCache {
   std::mutex mu;
-  bool attr_set[2][SW_MAX_NR + 1] = {};
+  bool attr_set[2][SW_MAX_NR + 1][2] = {};
 };
 LaunchCache g_cache;
 
-template <typename R, int NR>
-cudaError_t launch_nr(void* state, const SwSweep& sw, const DevPlan& dp, int sm_count,
+// Bulk copies pay off once a segment is long; shorter segments use direct loads.
+constexpr uint32_t kTmaMinSegmentBytes = 2048;
+
+template <typename R, int NR, bool kTma>
+cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_count,
                       cudaStream_t s) {
   using A = typename Amp<R>::type;
-  auto kern = k_sweep<R, NR>;
+  auto kern = k_sweep<R, NR, kTma>;
   const int di = std::is_same<R, float>::value ? 1 : 0;
   {
     std::lock_guard<std::mutex> lk(g_cache.mu);
-    if (!g_cache.attr_set[di][NR]) {
+    if (!g_cache.attr_set[di][NR][kTma]) {
       cudaError_t e =
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       if (e != cudaSuccess) return e;
-      g_cache.attr_set[di][NR] = true;
+      g_cache.attr_set[di][NR][kTma] = true;
     }
   }
-  const int threads = 1 << (sw.T - NR);
+  const int threads = 1 << (p.T - NR);
   if (threads > sweep_max_threads<R, NR>()) return cudaErrorInvalidConfiguration;
-  const size_t smem = (sw.s1 - sw.s0 > 1) ? (sizeof(A) << sw.T) : 0;
+  // bulk copies move whole 16-byte multiples from 16-byte aligned addresses
+  if (kTma && ((sizeof(A) << p.L) & 15u) != 0) return cudaErrorInvalidConfiguration;
+  const size_t smem = sweep_smem_bytes<R>(p.T, p.h, kTma, p.n_stages);
+  if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (e != cudaSuccess) return e;
   per_sm = std::max(per_sm, 1);
-  const int64_t grid = std::min<int64_t>(sw.tiles, (int64_t)sm_count * per_sm);
-  kern<<<(unsigned)grid, threads, smem, s>>>(static_cast<A*>(state), sw, dp.stages, dp.gates,
-                                             static_cast<const R*>(dp.pool));
+  const int64_t grid = std::min<int64_t>(p.tiles, (int64_t)sm_count * per_sm);
+  kern<<<(unsigned)grid, threads, smem, s>>>(static_cast<A*>(state), p, err);
   return cudaGetLastError();
 }
 
+template <typename R, int NR>
+cudaError_t launch_pick(void* state, const SweepParams<R>& p, int* err, int sm_count,
+                        cudaStream_t s) {
+  const uint32_t seg_bytes = (uint32_t)sizeof(typename Amp<R>::type) << p.L;
+  if (seg_bytes >= kTmaMinSegmentBytes) return launch_nr<R, NR, true>(state, p, err, sm_count, s);
+  return launch_nr<R, NR, false>(state, p, err, sm_count, s);
+}
+
 template <typename R>
-cudaError_t launch_t(void* state, const SwSweep& sw, const DevPlan& dp, int sm_count,
+cudaError_t launch_t(void* state, const SweepParams<R>& p, int* err, int sm_count,
                      cudaStream_t s) {
-  switch (sw.nr) {
-    case 1: return launch_nr<R, 1>(state, sw, dp, sm_count, s);
-    case 2: return launch_nr<R, 2>(state, sw, dp, sm_count, s);
-    case 3: return launch_nr<R, 3>(state, sw, dp, sm_count, s);
-    case 4: return launch_nr<R, 4>(state, sw, dp, sm_count, s);
+  switch (p.nr) {
+    case 1: return launch_pick<R, 1>(state, p, err, sm_count, s);
+    case 2: return launch_pick<R, 2>(state, p, err, sm_count, s);
+    case 3: return launch_pick<R, 3>(state, p, err, sm_count, s);
+    case 4: return launch_pick<R, 4>(state, p, err, sm_count, s);
     default: return cudaErrorInvalidValue;
   }
 }
 
+uint32_t host_spread(uint32_t x, const SwSweep& sw) {
+  uint32_t g = x & ((1u << sw.L) - 1u);
+  uint32_t hi = x >> sw.L;
+  for (int k = 0; hi; ++k, hi >>= 1)
+    if (hi & 1u) g |= 1u << sw.hq[k];
+  return g;
+}
+
+uint32_t host_swz(uint32_t i, int shift) { return i ^ ((i >> shift) & ((1u << shift) - 1u)); }
+
+// Copies sweep `k` of `plan` into the kernel-parameter form (sweep-local indices,
+// per-stage register tables).
+template <typename R>
+bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
+  const SwSweep& sw = plan.sweeps[k];
+  const int ns = sw.s1 - sw.s0;
+  if (ns < 1 || ns > kSweepMaxStages || sw.nr > SW_MAX_NR) return false;
+  const int g_lo = plan.stages[sw.s0].g0, g_hi = plan.stages[sw.s1 - 1].g1;
+  if (g_hi - g_lo > kSweepMaxGates) return false;
+  p->T = sw.T;
+  p->L = sw.L;
+  p->h = sw.h;
+  p->nr = sw.nr;
+  p->n_stages = ns;
+  p->pad = 0;
+  p->tiles = sw.tiles;
+  for (int q = 0; q < SW_MAX_HIGH; ++q) p->hq[q] = sw.hq[q];
+  const int shift = Amp<R>::kSwizzleShift;
+  const int nv = 1 << sw.nr;
+  for (int s = 0; s < ns; ++s) {
+    SwStage st = plan.stages[sw.s0 + s];
+    st.g0 -= g_lo;
+    st.g1 -= g_lo;
+    p->stages[s] = st;
+    for (int j = 0; j < 16; ++j) {
+      uint32_t o = 0;
+      if (j < nv)
+        for (int b = 0; b < sw.nr; ++b)
+          if (j & (1 << b)) o |= 1u << st.R[b];
+      p->tabs[s].off[j] = (uint16_t)o;
+      p->tabs[s].soff[j] = (uint16_t)host_swz(o, shift);
+    }
+  }
+  for (int j = 0; j < 16; ++j) {
+    p->gfirst[j] = host_spread(p->tabs[0].off[j], sw);
+    p->glast[j] = host_spread(p->tabs[ns - 1].off[j], sw);
+  }
+  const int32_t pool_lo = (g_hi > g_lo) ? plan.gates[g_lo].moff : 0;
+  for (int g = g_lo; g < g_hi; ++g) {
+    SwGate sg = plan.gates[g];
+    sg.moff -= pool_lo;
+    p->gates[g - g_lo] = sg;
+  }
+  // the pool slice of this sweep ends where the next sweep's first gate begins
+  int32_t pool_hi = (int32_t)plan.pool.size();
+  if (k + 1 < plan.sweeps.size()) {
+    const int next_g = plan.stages[plan.sweeps[k + 1].s0].g0;
+    if (next_g < (int)plan.gates.size()) pool_hi = plan.gates[next_g].moff;
+  }
+  if (pool_hi - pool_lo > kSweepMaxPool) return false;
+  for (int32_t e = pool_lo; e < pool_hi; ++e) p->pool[e - pool_lo] = (R)plan.pool[e];
+  return true;
+}
+
 }  // namespace
 
-cudaError_t launch_sweep(int dtype, void* state, int n, const SwSweep& sw, const DevPlan& dp,
+cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int* err,
                          int sm_count, cudaStream_t s) {
-  (void)n;
-  return dtype == SC_C64 ? launch_t<float>(state, sw, dp, sm_count, s)
-                         : launch_t<double>(state, sw, dp, sm_count, s);
+  if (dtype == SC_C64) {
+    SweepParams<float> p;
+    if (!fill_params(plan, k, &p)) return cudaErrorInvalidValue;
+    return launch_t<float>(state, p, err, sm_count, s);
+  }
+  SweepParams<double> p;
+  if (!fill_params(plan, k, &p)) return cudaErrorInvalidValue;
+  return launch_t<double>(state, p, err, sm_count, s);
 }
 
 }  // namespace sc

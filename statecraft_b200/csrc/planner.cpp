@@ -26,6 +26,16 @@ double gate_cost(const PGate& g) {
   }
 }
 
+int gate_pool_size(const PGate& g) {
+  switch (g.kind) {
+    case PK_DENSE1: return 8;
+    case PK_DENSE2: return 32;
+    case PK_DIAG1: return 4;
+    case PK_DIAG2: return 8;
+    default: return 0;
+  }
+}
+
 uint64_t dense_mask(const PGate& g) {
   switch (g.kind) {
     case PK_DENSE1:
@@ -230,6 +240,7 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     uint64_t H = 0;
     int hcount = 0;
     double used = 0.0;
+    int pool_used = 0;
     list.clear();
     for (int g = first; g < G; ++g) {
       if (when[g] >= 0) continue;
@@ -243,9 +254,11 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       const double cost = gate_cost(gates[g]);
       if (pp.budget >= 0 && !list.empty() && used + cost > pp.budget) break;
       if ((int)list.size() >= pp.max_gates) break;
+      if (pool_used + gate_pool_size(gates[g]) > pp.max_pool) break;
       H |= need;
       hcount += c;
       used += cost;
+      pool_used += gate_pool_size(gates[g]);
       when[g] = sweep_id;
       list.push_back(g);
     }
@@ -371,12 +384,20 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             sg.a = ref(pg.q0);
             plan.pool.insert(plan.pool.end(), pg.m, pg.m + 4);
             break;
-          case PK_DIAG2:
-            sg.kind = SK_D2;
+          case PK_DIAG2: {
             sg.a = ref(pg.q0);
             sg.b = ref(pg.q1);
-            plan.pool.insert(plan.pool.end(), pg.m, pg.m + 8);
+            const bool parity = pg.m[0] == pg.m[6] && pg.m[1] == pg.m[7] && pg.m[2] == pg.m[4] &&
+                                pg.m[3] == pg.m[5];
+            if (parity) {
+              sg.kind = SK_DP;
+              plan.pool.insert(plan.pool.end(), pg.m, pg.m + 4);
+            } else {
+              sg.kind = SK_D2;
+              plan.pool.insert(plan.pool.end(), pg.m, pg.m + 8);
+            }
             break;
+          }
         }
         plan.gates.push_back(sg);
         plan.gate_ops.push_back(pg.op_index);

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "sc_ctx.h"
+#include "sc_sweep.h"
 
 namespace sc {
 
@@ -229,56 +230,16 @@ uint64_t fresh_seed() {
 // ---------------------------------------------------------------------------
 namespace sc {
 
-int Ctx::upload_plan(const Plan& plan) {
-  const size_t st_bytes = std::max<size_t>(1, plan.stages.size()) * sizeof(SwStage);
-  const size_t g_bytes = std::max<size_t>(1, plan.gates.size()) * sizeof(SwGate);
-  const size_t rsize = (cfg.dtype == SC_C64) ? sizeof(float) : sizeof(double);
-  const size_t p_bytes = std::max<size_t>(1, plan.pool.size()) * rsize;
-  int rc;
-  if ((rc = reserve(buf_stages, st_bytes, "plan stages")) != SC_OK) return rc;
-  if ((rc = reserve(buf_gates, g_bytes, "plan gates")) != SC_OK) return rc;
-  if ((rc = reserve(buf_pool, p_bytes, "plan matrices")) != SC_OK) return rc;
-  // host staging buffer (pinned) holding stages | gates | pool
-  const size_t total = st_bytes + g_bytes + p_bytes;
-  if (total > staging_cap) {
-    if (staging) cudaFreeHost(staging);
-    staging = nullptr;
-    staging_cap = 0;
-    cudaError_t e = cudaMallocHost(&staging, total);
-    if (e != cudaSuccess) return fail_cuda(e, "cudaMallocHost(plan staging)");
-    staging_cap = total;
-  } else {
-    cudaStreamSynchronize(stream);  // previous plan copies have completed
-  }
-  char* h = static_cast<char*>(staging);
-  if (!plan.stages.empty()) std::memcpy(h, plan.stages.data(), plan.stages.size() * sizeof(SwStage));
-  if (!plan.gates.empty())
-    std::memcpy(h + st_bytes, plan.gates.data(), plan.gates.size() * sizeof(SwGate));
-  if (cfg.dtype == SC_C64) {
-    float* f = reinterpret_cast<float*>(h + st_bytes + g_bytes);
-    for (size_t k = 0; k < plan.pool.size(); ++k) f[k] = (float)plan.pool[k];
-  } else if (!plan.pool.empty()) {
-    std::memcpy(h + st_bytes + g_bytes, plan.pool.data(), plan.pool.size() * sizeof(double));
-  }
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(buf_stages.p, h, st_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-    return fail_cuda(e, "plan upload");
-  if ((e = cudaMemcpyAsync(buf_gates.p, h + st_bytes, g_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-    return fail_cuda(e, "plan upload");
-  if ((e = cudaMemcpyAsync(buf_pool.p, h + st_bytes + g_bytes, p_bytes, cudaMemcpyHostToDevice, stream)) != cudaSuccess)
-    return fail_cuda(e, "plan upload");
-  return SC_OK;
-}
-
 PlanParams Ctx::plan_params() const {
   PlanParams pp;
   const bool c64 = cfg.dtype == SC_C64;
-  pp.tile_qubits = cfg.tile_qubits > 0 ? cfg.tile_qubits : (c64 ? 12 : 11);
+  pp.tile_qubits = cfg.tile_qubits > 0 ? cfg.tile_qubits : (c64 ? 11 : 10);
   pp.low_qubits = low_qubits > 0 ? low_qubits : (c64 ? 5 : 4);
   pp.nr = nr > 0 ? nr : 3;
   pp.budget = cfg.sweep_budget > 0 ? (double)cfg.sweep_budget
                                    : (cfg.sweep_budget < 0 ? -1.0 : (c64 ? 160.0 : 96.0));
-  pp.max_gates = 4096;
+  pp.max_gates = kSweepMaxGates;
+  pp.max_pool = kSweepMaxPool;
   return pp;
 }
 
@@ -301,15 +262,10 @@ int Ctx::apply_gates(const std::vector<PGate>& gates) {
   }
   Plan plan = plan_sweeps(gates, n, plan_params());
   if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
-  int rc = upload_plan(plan);
-  if (rc != SC_OK) return rc;
-  DevPlan dp;
-  dp.stages = static_cast<SwStage*>(buf_stages.p);
-  dp.gates = static_cast<SwGate*>(buf_gates.p);
-  dp.pool = buf_pool.p;
-  for (const SwSweep& sw : plan.sweeps) {
+  for (size_t k = 0; k < plan.sweeps.size(); ++k) {
     mark_begin(KC_SWEEP, 2.0 * dim * amp_bytes);
-    cudaError_t e = launch_sweep(cfg.dtype, state.p, n, sw, dp, sm_count, stream);
+    cudaError_t e = launch_sweep(cfg.dtype, state.p, plan, k, static_cast<int*>(buf_err.p),
+                                 sm_count, stream);
     mark_end();
     if (e != cudaSuccess) return fail_cuda(e, "sweep kernel");
   }
@@ -341,6 +297,8 @@ int Ctx::run(int nq, const sc_op* ops, int64_t n_ops, const double* init, uint64
     return fail(SC_EINVAL, "basis-state qubit out of range");
   if ((rc = validate_channels(noise, ops, n_ops, nq)) != SC_OK) return rc;
   if ((rc = ensure_state(nq)) != SC_OK) return rc;
+  if ((rc = reserve(buf_err, 16, "error flag")) != SC_OK) return rc;
+  cudaMemsetAsync(buf_err.p, 0, 16, stream);
   plan_sweeps_count = plan_gates = plan_stages = 0;
 
   // state preparation (populateFromState / resetBasisState / resetZeroState)
@@ -430,6 +388,10 @@ int Ctx::run(int nq, const sc_op* ops, int64_t n_ops, const double* init, uint64
   cudaError_t e = cudaStreamSynchronize(stream);
   if (e != cudaSuccess) return fail_cuda(e, "sc_run");
   collect_timing();
+  int err_flag = 0;
+  if ((e = cudaMemcpy(&err_flag, buf_err.p, sizeof err_flag, cudaMemcpyDeviceToHost)) != cudaSuccess)
+    return fail_cuda(e, "error flag");
+  if (err_flag) return fail(SC_ETIMEOUT, "sweep kernel timed out waiting for a bulk copy");
   if (!noise.empty()) {
     NoiseDevState ns;
     e = cudaMemcpy(&ns, buf_noise_state.p, offsetof(NoiseDevState, choices), cudaMemcpyDeviceToHost);
@@ -476,7 +438,7 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
     return fail(SC_EINVAL, "dtype must be SC_C128 or SC_C64");
   }
   c->max_qubits = c->cfg.max_qubits > 0 ? c->cfg.max_qubits : SC_DEFAULT_MAX_QUBITS;
-  if (c->max_qubits > 40) c->max_qubits = 40;
+  if (c->max_qubits > SC_DEFAULT_MAX_QUBITS) c->max_qubits = SC_DEFAULT_MAX_QUBITS;
   if ((e = cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess ||
       (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) {
     delete c;
@@ -496,7 +458,6 @@ int32_t sc_destroy(void* p) {
   cudaStreamSynchronize(c->stream);
   c->release_all();
   for (cudaEvent_t ev : c->event_pool) cudaEventDestroy(ev);
-  if (c->staging) cudaFreeHost(c->staging);
   cudaStreamDestroy(c->stream);
   c->magic = 0;
   delete c;

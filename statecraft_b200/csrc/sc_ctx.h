@@ -43,15 +43,13 @@ struct Ctx {
 
   // device scratch (grow-only)
   size_t allocated = 0;
-  DevBuf buf_stages, buf_gates, buf_pool;       // sweep plan
+  DevBuf buf_err;                               // device error flag of bounded waits
   DevBuf buf_convert;                           // c64 <-> c128 staging
   DevBuf buf_noise_state, buf_noise_partial;    // Kraus trajectories
   DevBuf buf_sample;                            // chunk sums | prefix | scalars | uniforms | outcomes
   DevBuf buf_probs, buf_marg;                   // marginal probabilities
   DevBuf buf_expect;                            // Pauli partial sums
   DevBuf buf_adj_phi, buf_adj_lambda;           // adjoint work states
-  void* staging = nullptr;                      // pinned host staging for plan uploads
-  size_t staging_cap = 0;
 
   // adjoint bookkeeping
   std::vector<sc_op> adj_ops;
@@ -79,7 +77,7 @@ struct Ctx {
   int reserve(DevBuf& b, size_t bytes, const char* what);
   void release(DevBuf& b);
   void release_all() {
-    for (DevBuf* b : {&state, &buf_stages, &buf_gates, &buf_pool, &buf_convert, &buf_noise_state,
+    for (DevBuf* b : {&state, &buf_err, &buf_convert, &buf_noise_state,
                       &buf_noise_partial, &buf_sample, &buf_probs, &buf_marg, &buf_expect,
                       &buf_adj_phi, &buf_adj_lambda})
       release(*b);
@@ -90,7 +88,6 @@ struct Ctx {
   void collect_timing();
 
   PlanParams plan_params() const;
-  int upload_plan(const Plan& plan);
   int ensure_state(int nq);
   int apply_gates(const std::vector<PGate>& gates);
   int run(int nq, const sc_op* ops, int64_t n_ops, const double* init, uint64_t basis,

@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "sc_ctx.h"
+#include "sc_sweep.h"
 
 using namespace sc;
 
@@ -22,7 +23,8 @@ PlanParams debug_params(int tile, int low, int nr, double budget) {
   pp.low_qubits = low > 0 ? low : 4;
   pp.nr = nr > 0 ? nr : 3;
   pp.budget = budget;
-  pp.max_gates = 4096;
+  pp.max_gates = kSweepMaxGates;
+  pp.max_pool = kSweepMaxPool;
   return pp;
 }
 
@@ -145,6 +147,13 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
               for (int j = 0; j < NV; ++j) {
                 const uint32_t li = l0 | off[j];
                 const int k = (bitref_h(g.a, li, base) << 1) | bitref_h(g.b, li, base);
+                v[j] = cm(m[2 * k], m[2 * k + 1], v[j]);
+              }
+              break;
+            case SK_DP:
+              for (int j = 0; j < NV; ++j) {
+                const uint32_t li = l0 | off[j];
+                const int k = bitref_h(g.a, li, base) ^ bitref_h(g.b, li, base);
                 v[j] = cm(m[2 * k], m[2 * k + 1], v[j]);
               }
               break;

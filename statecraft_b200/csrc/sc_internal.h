@@ -50,7 +50,9 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 // Inside the tile, a stage gives each thread 2^NR amplitudes that differ in the
 // NR tile positions R[0..NR-1] (ascending); every gate of the stage acts on those
 // register bits (dense / permutation kinds) or on any bit (diagonal kinds).
-enum SwKind : int32_t { SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2 };
+// SK_DP: a two-qubit diagonal that depends only on the parity of its two bits
+// (diag(d0, d1, d1, d0), e.g. RZZ / exp(-i g ZZ)); pool holds d0, d1.
+enum SwKind : int32_t { SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP };
 
 constexpr int SW_MAX_HIGH = 24;
 constexpr int SW_MAX_NR = 4;
@@ -84,7 +86,11 @@ struct PlanParams {
   int nr;            // register qubits per stage
   double budget;     // FMA per amplitude per sweep; < 0 unlimited
   int max_gates;     // per sweep
+  int max_pool = 1 << 30;  // matrix reals per sweep
 };
+
+// matrix reals a normalised gate stores in the sweep pool
+int gate_pool_size(const PGate& g);
 
 struct Plan {
   std::vector<SwSweep> sweeps;
@@ -122,17 +128,11 @@ const char* kernel_class_name(int cls);
 // ---------------------------------------------------------------------------
 // launchers (implemented in the .cu files; all asynchronous on `stream`)
 // ---------------------------------------------------------------------------
-struct DevPlan {
-  SwStage* stages = nullptr;
-  SwGate* gates = nullptr;
-  void* pool = nullptr;   // double (c128) or float (c64)
-  size_t cap_stages = 0, cap_gates = 0, cap_pool = 0;
-};
-
 // per-gate path (fusion off); `state` is double2* or float2* per dtype
 cudaError_t launch_gate(int dtype, void* state, int n, const PGate& g, cudaStream_t s);
-// fused sweep
-cudaError_t launch_sweep(int dtype, void* state, int n, const SwSweep& sw, const DevPlan& dp,
+// fused sweep number k of `plan` (n <= 32); `err` (device int) is set to 1 if a
+// bulk-copy wait times out
+cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int* err,
                          int sm_count, cudaStream_t s);
 // |0..0> or |basis>
 cudaError_t launch_init_basis(int dtype, void* state, int n, uint64_t basis, cudaStream_t s);

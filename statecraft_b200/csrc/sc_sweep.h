@@ -1,0 +1,39 @@
+// Kernel-parameter form of one fused sweep (k_sweep.cu).
+#pragma once
+
+#include <stdint.h>
+
+#include "sc_internal.h"
+
+namespace sc {
+
+// A sweep's plan travels as one __grid_constant__ kernel parameter (< 32 KB).
+constexpr int kSweepMaxStages = 96;
+constexpr int kSweepMaxGates = 94;   // stages <= gates + 2
+constexpr int kSweepMaxPool = 2048;  // matrix reals
+
+// Per-stage register tables computed on the host: off[j] is the tile offset of
+// register j (the OR of 1 << R[k] over the set bits k of j) and soff[j] its
+// swizzled shared-memory slot (the swizzle is XOR-linear over disjoint bits).
+struct SwStageTab {
+  uint16_t off[16];
+  uint16_t soff[16];
+};
+
+template <typename R>
+struct SweepParams {
+  int32_t T, L, h, nr;
+  int32_t n_stages, pad;
+  int64_t tiles;
+  int32_t hq[SW_MAX_HIGH];
+  uint32_t gfirst[16];  // global offset of register j in the first stage's layout
+  uint32_t glast[16];   // ... and in the last stage's layout
+  SwStage stages[kSweepMaxStages];
+  SwStageTab tabs[kSweepMaxStages];
+  SwGate gates[kSweepMaxGates];
+  R pool[kSweepMaxPool];
+};
+
+static_assert(sizeof(SweepParams<double>) < 32000, "sweep parameters must fit the 32 KB limit");
+
+}  // namespace sc
