@@ -117,6 +117,9 @@ SIGNATURES = {
     "sc_kernel_class_name": (ctypes.c_char_p, [ctypes.c_int32]),
     "sc_reset_kernel_stats": (ctypes.c_int32, [ctypes.c_void_p]),
     "sc_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "sc_sample_static": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32,
+                                          ctypes.c_int64, ctypes.c_uint64, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "sc_last_plan_stats": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int64),
                                             _P(ctypes.c_int64), _P(ctypes.c_int64)]),
     "sc_debug_plan_order": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
