@@ -53,6 +53,16 @@ __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R*
 template <typename R, int NR, int A_>
 __device__ __forceinline__ void xswap(typename Amp<R>::type (&v)[1 << NR], uint32_t l0,
                                       const uint32_t (&off)[1 << NR], uint32_t lmask) {
+  if (lmask == 0) {  // no control inside the tile: a plain register permutation
+#pragma unroll
+    for (int j = 0; j < (1 << NR); ++j) {
+      if (j & (1 << A_)) continue;
+      const auto t = v[j];
+      v[j] = v[j | (1 << A_)];
+      v[j | (1 << A_)] = t;
+    }
+    return;
+  }
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j) {
     if (j & (1 << A_)) continue;
@@ -61,6 +71,39 @@ __device__ __forceinline__ void xswap(typename Amp<R>::type (&v)[1 << NR], uint3
     const auto a0 = v[j], a1 = v[j1];
     v[j] = on ? a1 : a0;
     v[j1] = on ? a0 : a1;
+  }
+}
+
+// controlled X with target register bit T_ and control register bit C_; further
+// controls (lmask) lie on tile positions outside the registers, so their test is
+// the same for all of a thread's registers
+template <typename R, int NR, int T_, int C_>
+__device__ __forceinline__ void cxswap(typename Amp<R>::type (&v)[1 << NR], uint32_t l0,
+                                       uint32_t lmask) {
+  const bool on = (l0 & lmask) == lmask;
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    if ((j & (1 << T_)) || !(j & (1 << C_))) continue;
+    const int j1 = j | (1 << T_);
+    const auto a0 = v[j], a1 = v[j1];
+    if (lmask == 0) {
+      v[j] = a1;
+      v[j1] = a0;
+    } else {
+      v[j] = on ? a1 : a0;
+      v[j1] = on ? a0 : a1;
+    }
+  }
+}
+
+// parity diagonal on register bits A_, B_: factor d[bit A_ ^ bit B_], fixed per register
+template <typename R, int NR, int A_, int B_>
+__device__ __forceinline__ void dpr(typename Amp<R>::type (&v)[1 << NR], const R* m) {
+  const R d0r = m[0], d0i = m[1], d1r = m[2], d1i = m[3];
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const int par = ((j >> A_) ^ (j >> B_)) & 1;
+    v[j] = par ? cmul(d1r, d1i, v[j]) : cmul(d0r, d0i, v[j]);
   }
 }
 
@@ -122,6 +165,59 @@ __device__ __forceinline__ void dispatch2(int a, int b, F&& f) {
     });
   });
 }
+
+// X on register bit A_ with no tile controls outside the registers
+template <typename R, int NR, int A_>
+__device__ __forceinline__ void xswap0(typename Amp<R>::type (&v)[1 << NR]) {
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    if (j & (1 << A_)) continue;
+    const auto t = v[j];
+    v[j] = v[j | (1 << A_)];
+    v[j | (1 << A_)] = t;
+  }
+}
+
+// controlled X, target register bit T_, control register bit C_, no other tile controls
+template <typename R, int NR, int T_, int C_>
+__device__ __forceinline__ void cxswap0(typename Amp<R>::type (&v)[1 << NR]) {
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    if ((j & (1 << T_)) || !(j & (1 << C_))) continue;
+    const auto t = v[j];
+    v[j] = v[j | (1 << T_)];
+    v[j | (1 << T_)] = t;
+  }
+}
+
+// uncontrolled diag(d0, d1) on register bit A_: the factor of each register is fixed
+template <typename R, int NR, int A_>
+__device__ __forceinline__ void d1r(typename Amp<R>::type (&v)[1 << NR], const R* m) {
+  const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j)
+    v[j] = ((j >> A_) & 1) ? cmul(d1r_, d1i_, v[j]) : cmul(d0r, d0i, v[j]);
+}
+
+// switch cases for the dispatch code (sw_code): one jump per gate into code that
+// is specialised on its register bits
+#define SC_CASE_1(K, A, F) \
+  case ((K) << 4) | ((A) << 2):  \
+    if constexpr ((A) < NR) {    \
+      F(A);                      \
+    }                            \
+    break;
+#define SC_CASES_1(K, F) SC_CASE_1(K, 0, F) SC_CASE_1(K, 1, F) SC_CASE_1(K, 2, F) SC_CASE_1(K, 3, F)
+#define SC_CASE_2(K, A, B, F)              \
+  case ((K) << 4) | ((A) << 2) | (B):      \
+    if constexpr ((A) < NR && (B) < NR) {  \
+      F(A, B);                             \
+    }                                      \
+    break;
+#define SC_CASES_2(K, F)                                                                  \
+  SC_CASE_2(K, 0, 1, F) SC_CASE_2(K, 0, 2, F) SC_CASE_2(K, 0, 3, F) SC_CASE_2(K, 1, 0, F) \
+  SC_CASE_2(K, 1, 2, F) SC_CASE_2(K, 1, 3, F) SC_CASE_2(K, 2, 0, F) SC_CASE_2(K, 2, 1, F) \
+  SC_CASE_2(K, 2, 3, F) SC_CASE_2(K, 3, 0, F) SC_CASE_2(K, 3, 1, F) SC_CASE_2(K, 3, 2, F)
 
 // local tile index -> global offset (n <= 32: 32-bit)
 template <typename P>
@@ -271,18 +367,15 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
       const uint32_t sw0 = swz<R>(nl0);
       if (s > 0) {
         __syncthreads();  // readers of the buffer are done
+        // sidx: the previous stage's exit slots (its folded permutation applied)
 #pragma unroll
         for (int j = 0; j < NV; ++j) cur[sidx[j]] = v[j];
         __syncthreads();
 #pragma unroll
-        for (int j = 0; j < NV; ++j) {
-          sidx[j] = sw0 ^ tab.soff[j];
-          v[j] = cur[sidx[j]];
-        }
-      } else {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.soff[j];
+        for (int j = 0; j < NV; ++j) v[j] = cur[sw0 ^ tab.soff[j]];
       }
+#pragma unroll
+      for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.wsoff[j];
       l0 = nl0;
 #pragma unroll
       for (int j = 0; j < NV; ++j) off[j] = tab.off[j];
@@ -293,62 +386,88 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
         if (((uint64_t)base & g.gmask) != g.gmask) continue;
         const R* m = p.pool + g.moff;
         const uint32_t lmask = g.lmask;
-        switch (g.kind) {
-          case SK_G1:
-            dispatch1<NR>(g.a, [&](auto ia) { g1<R, NR, decltype(ia)::value>(v, m, l0, off, lmask); });
-            break;
-          case SK_X:
-            dispatch1<NR>(g.a, [&](auto ia) { xswap<R, NR, decltype(ia)::value>(v, l0, off, lmask); });
-            break;
-          case SK_G2:
+        switch (g.code) {
+#define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask)
+#define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask)
+#define SC_DO_D1R(A) d1r<R, NR, A>(v, m)
+#define SC_DO_G2(A, B) g2<R, NR, A, B>(v, m)
+#define SC_DO_CX(A, B) cxswap<R, NR, A, B>(v, l0, lmask)
+#define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m)
+#define SC_DO_SWAP(A, B) rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v)
+#define SC_DO_X0(A) xswap0<R, NR, A>(v)
+#define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v)
+          SC_CASES_1(SK_X0, SC_DO_X0)
+          SC_CASES_2(SK_CX0, SC_DO_CX0)
+#undef SC_DO_X0
+#undef SC_DO_CX0
+          SC_CASES_1(SK_G1, SC_DO_G1)
+          SC_CASES_1(SK_X, SC_DO_X)
+          SC_CASES_1(SK_D1R, SC_DO_D1R)
+          SC_CASES_2(SK_G2, SC_DO_G2)
+          SC_CASES_2(SK_CX, SC_DO_CX)
+          SC_CASES_2(SK_DPR, SC_DO_DPR)
+          SC_CASES_2(SK_SWAP, SC_DO_SWAP)
+#undef SC_DO_G1
+#undef SC_DO_X
+#undef SC_DO_D1R
+#undef SC_DO_G2
+#undef SC_DO_CX
+#undef SC_DO_DPR
+#undef SC_DO_SWAP
+          case SK_G1ALL << 4: {
+            // commuting 2x2 gates on several register bits, matrices in bit order
+            const int mask = g.a;
+            const R* mm = m;
+            if (mask & 1) {
+              g1<R, NR, 0>(v, mm, l0, off, 0u);
+              mm += 8;
+            }
             if constexpr (NR > 1)
-              dispatch2<NR>(g.a, g.b, [&](auto ia, auto ib) {
-                g2<R, NR, decltype(ia)::value, decltype(ib)::value>(v, m);
-              });
+              if (mask & 2) {
+                g1<R, NR, 1>(v, mm, l0, off, 0u);
+                mm += 8;
+              }
+            if constexpr (NR > 2)
+              if (mask & 4) {
+                g1<R, NR, 2>(v, mm, l0, off, 0u);
+                mm += 8;
+              }
+            if constexpr (NR > 3)
+              if (mask & 8) g1<R, NR, 3>(v, mm, l0, off, 0u);
             break;
-          case SK_SWAP:
-            if constexpr (NR > 1)
-              dispatch2<NR>(g.a, g.b, [&](auto ia, auto ib) {
-                constexpr int kA = decltype(ia)::value;
-                constexpr int kB = decltype(ib)::value;
-                if constexpr (kA < kB)
-                  rswap<R, NR, kA, kB>(v);
-                else
-                  rswap<R, NR, kB, kA>(v);
-              });
-            break;
-          case SK_D1: {
+          }
+          case SK_D1 << 4: {
             // diag(d0, d1) on one bit; the bit is a tile position (a >= 0) or a
             // global qubit fixed for the whole tile (a < 0)
             const int a = g.a;
             const uint32_t gb = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
             const int sh = a < 0 ? 0 : a;
             const uint32_t lm = a < 0 ? 0u : 1u;
-            const R d0r = m[0], d0i = m[1], d1r = m[2], d1i = m[3];
+            const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
               const uint32_t li = l0 | off[j];
               if ((li & lmask) != lmask) continue;
               const uint32_t bit = ((li >> sh) & lm) | gb;
-              v[j] = cmul(bit ? d1r : d0r, bit ? d1i : d0i, v[j]);
+              v[j] = cmul(bit ? d1r_ : d0r, bit ? d1i_ : d0i, v[j]);
             }
             break;
           }
-          case SK_DP: {
+          case SK_DP << 4: {
             // parity diagonal: factor d[bit(a) ^ bit(b)]
             const int a = g.a, bq = g.b;
             const uint32_t gpar = (a < 0 ? ((base >> (-a - 1)) & 1u) : 0u) ^
                                   (bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u);
             const uint32_t pm = (a < 0 ? 0u : (1u << a)) | (bq < 0 ? 0u : (1u << bq));
-            const R d0r = m[0], d0i = m[1], d1r = m[2], d1i = m[3];
+            const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
 #pragma unroll
             for (int j = 0; j < NV; ++j) {
               const uint32_t bit = (__popc((l0 | off[j]) & pm) & 1u) ^ gpar;
-              v[j] = cmul(bit ? d1r : d0r, bit ? d1i : d0i, v[j]);
+              v[j] = cmul(bit ? d1r_ : d0r, bit ? d1i_ : d0i, v[j]);
             }
             break;
           }
-          case SK_D2: {
+          case SK_D2 << 4: {
             const int a = g.a, bq = g.b;
             const uint32_t ga = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
             const uint32_t gbb = bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u;
@@ -370,9 +489,8 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
       // stage the results in the linear layout and drain them with bulk stores
       __syncthreads();  // every read of `cur` is done
       {
-        const SwStageTab& tab = p.tabs[ns - 1];
 #pragma unroll
-        for (int j = 0; j < NV; ++j) cur[l0_last | tab.off[j]] = v[j];
+        for (int j = 0; j < NV; ++j) cur[l0_last | p.lastoff[j]] = v[j];
       }
       fence_proxy_async_smem();
       __syncthreads();
@@ -500,10 +618,18 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
       p->tabs[s].off[j] = (uint16_t)o;
       p->tabs[s].soff[j] = (uint16_t)host_swz(o, shift);
     }
+    for (int j = 0; j < 16; ++j) {
+      const int pj = (j < nv) ? st.perm[j] : j;
+      if (pj < 0 || pj >= 16) return false;
+      p->tabs[s].wsoff[j] = p->tabs[s].soff[pj];
+    }
   }
+  const SwStage& last = p->stages[ns - 1];
   for (int j = 0; j < 16; ++j) {
+    const int pj = (j < nv) ? last.perm[j] : j;
     p->gfirst[j] = host_spread(p->tabs[0].off[j], sw);
-    p->glast[j] = host_spread(p->tabs[ns - 1].off[j], sw);
+    p->lastoff[j] = p->tabs[ns - 1].off[pj];
+    p->glast[j] = host_spread(p->lastoff[j], sw);
   }
   const int32_t pool_lo = (g_hi > g_lo) ? plan.gates[g_lo].moff : 0;
   for (int g = g_lo; g < g_hi; ++g) {

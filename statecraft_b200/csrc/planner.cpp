@@ -207,6 +207,11 @@ Dag build_dag(const std::vector<PGate>& gates, int n) {
 
 inline int popc(uint64_t x) { return __builtin_popcountll(x); }
 
+// diag(d0, d1, d1, d0): depends only on the parity of the two bits
+bool is_parity_diag(const PGate& g) {
+  return g.m[0] == g.m[6] && g.m[1] == g.m[7] && g.m[2] == g.m[4] && g.m[3] == g.m[5];
+}
+
 }  // namespace
 
 Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
@@ -283,6 +288,7 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       }
     }
     const uint32_t high_pos = (T >= 32 ? 0xFFFFFFFFu : ((1u << T) - 1u)) & ~((1u << L) - 1u);
+    const uint64_t tile_qmask = low_qmask | H;
 
     // ---- stages -----------------------------------------------------------
     for (size_t i = 0; i < list.size(); ++i) idx_in_sweep[list[i]] = (int32_t)i;
@@ -290,9 +296,12 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     size_t remaining = list.size();
     sw.s0 = (int32_t)plan.stages.size();
     std::vector<std::pair<uint32_t, std::vector<int32_t>>> stage_list;
+    // folded[i]: list gate i is a permutation folded into its stage's exit permutation
+    std::vector<char> folded(list.size(), 0);
     while (remaining > 0 || stage_list.empty()) {
       const bool first_stage = stage_list.empty();
       uint32_t R = 0;
+      uint32_t frozen = 0;  // positions moved by a folded permutation of this stage
       std::vector<int32_t> sg;
       for (size_t i = 0; i < list.size(); ++i) {
         if (staged[i]) continue;
@@ -303,13 +312,54 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
           if (when[dpd] == sweep_id && !staged[idx_in_sweep[dpd]]) { ok = false; break; }
         }
         if (!ok) continue;
+        uint32_t touch = 0;
+        for (uint64_t m = touch_mask(gates[g]); m; m &= m - 1) {
+          const int q = __builtin_ctzll(m);
+          if (pos_of[q] >= 0) touch |= 1u << pos_of[q];
+        }
+        // data on frozen positions has logically moved already: wait for the next stage
+        if (touch & frozen) continue;
         uint32_t need = 0;
         for (uint64_t m = dense_mask(gates[g]); m; m &= m - 1)
           need |= 1u << pos_of[__builtin_ctzll(m)];
         need &= ~R;
         if (first_stage && high_edges && (need & ~high_pos)) continue;
         if (popc(R) + popc(need) > NR) continue;
+        // Positions that make the gate cheaper when they are register bits too: the
+        // control of a controlled X (a register permutation) and both bits of a
+        // parity diagonal (a compile-time phase pattern).  Taken only if they fit.
+        uint32_t want = 0;
+        const PGate& pw = gates[g];
+        if (pw.kind == PK_X) {
+          for (uint64_t m = pw.cmask; m; m &= m - 1) {
+            const int c = __builtin_ctzll(m);
+            if (pos_of[c] >= 0) {
+              want |= 1u << pos_of[c];
+              break;
+            }
+          }
+        } else if (pw.kind == PK_DIAG2 && is_parity_diag(pw) && pos_of[pw.q0] >= 0 &&
+                   pos_of[pw.q1] >= 0) {
+          want = (1u << pos_of[pw.q0]) | (1u << pos_of[pw.q1]);
+        } else if (pw.kind == PK_DIAG1 && pw.cmask == 0 && pos_of[pw.q0] >= 0) {
+          want = 1u << pos_of[pw.q0];
+        }
+        want &= ~R & ~need;
+        if (first_stage && high_edges) want &= high_pos;
+        if (popc(R) + popc(need) + popc(want) <= NR) need |= want;
         R |= need;
+        // X / CNOT / SWAP acting only on register bits is a register permutation:
+        // fold it into the stage's exit permutation instead of moving data
+        bool fold = false;
+        if (pw.kind == PK_SWAP) {
+          fold = true;
+        } else if (pw.kind == PK_X && (pw.cmask & ~tile_qmask) == 0 && popc(pw.cmask) <= 1) {
+          fold = pw.cmask == 0 || ((touch & ~R) == 0);
+        }
+        if (fold) {
+          folded[i] = 1;
+          frozen |= touch;
+        }
         sg.push_back((int32_t)i);
         staged[i] = 1;
       }
@@ -347,8 +397,70 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         }
       }
       st.g0 = (int32_t)plan.gates.size();
+      for (int j = 0; j < 16; ++j) st.perm[j] = (int8_t)j;
+      std::vector<int64_t> folded_ops;
+      // runs of uncontrolled 2x2 gates on distinct register bits become one record
+      std::vector<std::pair<int, const double*>> run;
+      std::vector<int64_t> run_ops;
+      auto flush_run = [&]() {
+        if (run.empty()) return;
+        SwGate sg;
+        std::memset(&sg, 0, sizeof sg);
+        sg.moff = (int32_t)plan.pool.size();
+        if (run.size() == 1) {
+          sg.kind = SK_G1;
+          sg.a = run[0].first;
+          plan.pool.insert(plan.pool.end(), run[0].second, run[0].second + 8);
+        } else {
+          std::sort(run.begin(), run.end(),
+                    [](const std::pair<int, const double*>& x, const std::pair<int, const double*>& y) {
+                      return x.first < y.first;
+                    });
+          sg.kind = SK_G1ALL;
+          for (const auto& r : run) {
+            sg.a |= 1 << r.first;
+            plan.pool.insert(plan.pool.end(), r.second, r.second + 8);
+          }
+        }
+        sg.code = sw_code(sg.kind, sg.a, sg.b);
+        plan.gates.push_back(sg);
+        plan.gate_ops.insert(plan.gate_ops.end(), run_ops.begin(), run_ops.end());
+        run.clear();
+        run_ops.clear();
+      };
       for (int32_t li : stage_list[s].second) {
         const PGate& pg = gates[list[li]];
+        if (folded[li]) {
+          // compose the register map of the permutation onto the exit permutation
+          const int ta = reg_of_pos[pos_of[pg.q0]];
+          int cb = -1, sb = -1;
+          if (pg.kind == PK_SWAP) sb = reg_of_pos[pos_of[pg.q1]];
+          else if (pg.cmask) cb = reg_of_pos[pos_of[__builtin_ctzll(pg.cmask)]];
+          for (int j = 0; j < (1 << NR); ++j) {
+            int x = st.perm[j];
+            if (pg.kind == PK_SWAP) {
+              const int ba = (x >> ta) & 1, bb = (x >> sb) & 1;
+              if (ba != bb) x ^= (1 << ta) | (1 << sb);
+            } else if (cb < 0 || ((x >> cb) & 1)) {
+              x ^= 1 << ta;
+            }
+            st.perm[j] = (int8_t)x;
+          }
+          folded_ops.push_back(pg.op_index);
+          continue;
+        }
+        if (pg.kind == PK_DENSE1 && pg.cmask == 0) {
+          const int bit = reg_of_pos[pos_of[pg.q0]];
+          for (const auto& r : run)
+            if (r.first == bit) {
+              flush_run();
+              break;
+            }
+          run.emplace_back(bit, pg.m);
+          run_ops.push_back(pg.op_index);
+          continue;
+        }
+        flush_run();
         SwGate sg;
         std::memset(&sg, 0, sizeof sg);
         for (uint64_t m = pg.cmask; m; m &= m - 1) {
@@ -370,10 +482,24 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             sg.b = reg_of_pos[pos_of[pg.q1]];
             plan.pool.insert(plan.pool.end(), pg.m, pg.m + 32);
             break;
-          case PK_X:
+          case PK_X: {
             sg.kind = SK_X;
             sg.a = reg_of_pos[pos_of[pg.q0]];
+            // a control that is a register bit turns the gate into a register permutation
+            for (uint64_t m = pg.cmask; m; m &= m - 1) {
+              const int c = __builtin_ctzll(m);
+              if (pos_of[c] >= 0 && reg_of_pos[pos_of[c]] >= 0) {
+                // the remaining tile controls must lie outside the registers
+                const uint32_t rest = sg.lmask & ~(1u << pos_of[c]);
+                if (rest & R) break;
+                sg.kind = SK_CX;
+                sg.b = reg_of_pos[pos_of[c]];
+                sg.lmask = rest;
+                break;
+              }
+            }
             break;
+          }
           case PK_SWAP:
             sg.kind = SK_SWAP;
             sg.a = reg_of_pos[pos_of[pg.q0]];
@@ -382,15 +508,22 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
           case PK_DIAG1:
             sg.kind = SK_D1;
             sg.a = ref(pg.q0);
+            if (pg.cmask == 0 && sg.a >= 0 && reg_of_pos[sg.a] >= 0) {
+              sg.kind = SK_D1R;
+              sg.a = reg_of_pos[sg.a];
+            }
             plan.pool.insert(plan.pool.end(), pg.m, pg.m + 4);
             break;
           case PK_DIAG2: {
             sg.a = ref(pg.q0);
             sg.b = ref(pg.q1);
-            const bool parity = pg.m[0] == pg.m[6] && pg.m[1] == pg.m[7] && pg.m[2] == pg.m[4] &&
-                                pg.m[3] == pg.m[5];
-            if (parity) {
+            if (is_parity_diag(pg)) {
               sg.kind = SK_DP;
+              if (sg.a >= 0 && sg.b >= 0 && reg_of_pos[sg.a] >= 0 && reg_of_pos[sg.b] >= 0) {
+                sg.kind = SK_DPR;
+                sg.a = reg_of_pos[sg.a];
+                sg.b = reg_of_pos[sg.b];
+              }
               plan.pool.insert(plan.pool.end(), pg.m, pg.m + 4);
             } else {
               sg.kind = SK_D2;
@@ -399,9 +532,14 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             break;
           }
         }
+        if (sg.kind == SK_X && sg.lmask == 0) sg.kind = SK_X0;
+        if (sg.kind == SK_CX && sg.lmask == 0) sg.kind = SK_CX0;
+        sg.code = sw_code(sg.kind, sg.a, sg.b);
         plan.gates.push_back(sg);
         plan.gate_ops.push_back(pg.op_index);
       }
+      flush_run();
+      plan.gate_ops.insert(plan.gate_ops.end(), folded_ops.begin(), folded_ops.end());
       st.g1 = (int32_t)plan.gates.size();
       plan.stages.push_back(st);
     }

@@ -69,7 +69,7 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
   const uint32_t threads = 1u << (sw.T - NR);
   std::vector<C> v(NV);
   std::vector<uint32_t> off(NV);
-  std::vector<uint64_t> gidx(NV);
+  std::vector<uint64_t> gidx(NV), out(NV);
   for (int64_t t = 0; t < sw.tiles; ++t) {
     uint64_t base = (uint64_t)t << sw.L;
     for (int k = 0; k < sw.h; ++k) {
@@ -98,6 +98,14 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
           const double* m = plan.pool.data() + g.moff;
           auto ok = [&](int j) { return ((l0 | off[j]) & g.lmask) == g.lmask; };
           switch (g.kind) {
+            case SK_X0:
+              for (int j = 0; j < NV; ++j)
+                if (!(j & (1 << g.a))) std::swap(v[j], v[j | (1 << g.a)]);
+              break;
+            case SK_CX0:
+              for (int j = 0; j < NV; ++j)
+                if (!(j & (1 << g.a)) && (j & (1 << g.b))) std::swap(v[j], v[j | (1 << g.a)]);
+              break;
             case SK_G1:
             case SK_X:
               for (int j = 0; j < NV; ++j) {
@@ -150,6 +158,40 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
                 v[j] = cm(m[2 * k], m[2 * k + 1], v[j]);
               }
               break;
+            case SK_G1ALL: {
+              const double* mm = m;
+              for (int bit = 0; bit < NR; ++bit) {
+                if (!((g.a >> bit) & 1)) continue;
+                for (int j = 0; j < NV; ++j) {
+                  if (j & (1 << bit)) continue;
+                  const int j1 = j | (1 << bit);
+                  const C a0 = v[j], a1 = v[j1];
+                  v[j] = mac2(mm + 0, a0, mm + 2, a1);
+                  v[j1] = mac2(mm + 4, a0, mm + 6, a1);
+                }
+                mm += 8;
+              }
+              break;
+            }
+            case SK_D1R:
+              for (int j = 0; j < NV; ++j) {
+                const int k = (j >> g.a) & 1;
+                v[j] = cm(m[2 * k], m[2 * k + 1], v[j]);
+              }
+              break;
+            case SK_CX:
+              for (int j = 0; j < NV; ++j) {
+                if ((j & (1 << g.a)) || !(j & (1 << g.b))) continue;
+                if ((l0 & g.lmask) != g.lmask) continue;
+                std::swap(v[j], v[j | (1 << g.a)]);
+              }
+              break;
+            case SK_DPR:
+              for (int j = 0; j < NV; ++j) {
+                const int k = ((j >> g.a) ^ (j >> g.b)) & 1;
+                v[j] = cm(m[2 * k], m[2 * k + 1], v[j]);
+              }
+              break;
             case SK_DP:
               for (int j = 0; j < NV; ++j) {
                 const uint32_t li = l0 | off[j];
@@ -159,9 +201,14 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
               break;
           }
         }
+        // folded permutations: register j leaves the stage as register perm[j]
         for (int j = 0; j < NV; ++j) {
-          st[2 * gidx[j]] = v[j].r;
-          st[2 * gidx[j] + 1] = v[j].i;
+          const uint64_t dst = gidx[stg.perm[j]];
+          out[j] = dst;
+        }
+        for (int j = 0; j < NV; ++j) {
+          st[2 * out[j]] = v[j].r;
+          st[2 * out[j] + 1] = v[j].i;
         }
       }
     }

@@ -52,7 +52,29 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 // register bits (dense / permutation kinds) or on any bit (diagonal kinds).
 // SK_DP: a two-qubit diagonal that depends only on the parity of its two bits
 // (diag(d0, d1, d1, d0), e.g. RZZ / exp(-i g ZZ)); pool holds d0, d1.
-enum SwKind : int32_t { SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP };
+// SK_CX: controlled X whose target (a) and one control (b) are register bits; any
+//        other controls are tile positions outside the registers (lmask) or global.
+// SK_DPR: SK_DP whose two bits are register bits a, b.
+// SK_G1ALL: uncontrolled 2x2 gates on several distinct register bits (bit mask in a),
+//        matrices in the pool in increasing bit order; they commute, so one record.
+// SK_D1R: uncontrolled diag(d0, d1) on register bit a.
+// SK_X0 / SK_CX0: SK_X / SK_CX without controls on tile positions outside the
+//        registers (a fixed register permutation).
+enum SwKind : int32_t {
+  SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
+  SK_X0, SK_CX0
+};
+
+// Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
+// register bits (< 4), kind << 4 otherwise.  The kernel switches on it once.
+inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
+  switch (kind) {
+    case SK_G1: case SK_X: case SK_D1R: case SK_X0: return (kind << 4) | (a << 2);
+    case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0:
+      return (kind << 4) | (a << 2) | b;
+    default: return kind << 4;
+  }
+}
 
 constexpr int SW_MAX_HIGH = 24;
 constexpr int SW_MAX_NR = 4;
@@ -63,14 +85,18 @@ struct SwGate {     // 32 bytes
                     //   ref >= 0 -> tile position, ref < 0 -> global qubit (-ref - 1)
   int32_t moff;     // offset of the matrix in the sweep pool (reals)
   uint32_t lmask;   // control bits on tile positions
-  uint32_t pad;
+  int32_t code;     // sw_code(kind, a, b)
   uint64_t gmask;   // control bits on global (non-tile) qubits
 };
 
-struct SwStage {    // 16 bytes
+struct SwStage {    // 32 bytes
   int32_t g0, g1;   // gate range
   int8_t R[SW_MAX_NR];
   int32_t nr;       // number of meaningful register positions (== kernel NR)
+  // Exit permutation of the registers: permutation gates on register bits (X,
+  // CNOT, SWAP) are not executed but folded here; the data of register j leaves
+  // the stage as register perm[j] (through the next exchange or the final store).
+  int8_t perm[16];
 };
 
 struct SwSweep {

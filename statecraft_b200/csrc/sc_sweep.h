@@ -8,16 +8,18 @@
 namespace sc {
 
 // A sweep's plan travels as one __grid_constant__ kernel parameter (< 32 KB).
-constexpr int kSweepMaxStages = 96;
-constexpr int kSweepMaxGates = 94;   // stages <= gates + 2
+constexpr int kSweepMaxStages = 80;
+constexpr int kSweepMaxGates = 78;   // stages <= gates + 2
 constexpr int kSweepMaxPool = 2048;  // matrix reals
 
 // Per-stage register tables computed on the host: off[j] is the tile offset of
-// register j (the OR of 1 << R[k] over the set bits k of j) and soff[j] its
-// swizzled shared-memory slot (the swizzle is XOR-linear over disjoint bits).
+// register j (the OR of 1 << R[k] over the set bits k of j), soff[j] its swizzled
+// shared-memory slot (the swizzle is XOR-linear over disjoint bits) and wsoff[j]
+// the slot register j is written to when the stage ends (soff[perm[j]]).
 struct SwStageTab {
   uint16_t off[16];
   uint16_t soff[16];
+  uint16_t wsoff[16];
 };
 
 template <typename R>
@@ -26,8 +28,9 @@ struct SweepParams {
   int32_t n_stages, pad;
   int64_t tiles;
   int32_t hq[SW_MAX_HIGH];
-  uint32_t gfirst[16];  // global offset of register j in the first stage's layout
-  uint32_t glast[16];   // ... and in the last stage's layout
+  uint32_t gfirst[16];   // global offset of register j in the first stage's layout
+  uint32_t glast[16];    // global offset register j is stored to (last stage, perm applied)
+  uint16_t lastoff[16];  // tile offset register j is stored to (last stage, perm applied)
   SwStage stages[kSweepMaxStages];
   SwStageTab tabs[kSweepMaxStages];
   SwGate gates[kSweepMaxGates];
