@@ -142,6 +142,33 @@ __device__ __forceinline__ void bulk_wait_all() {
 }
 
 // orders this thread's generic-proxy shared-memory accesses with async-proxy (TMA) ones
+__device__ __forceinline__ void prefetch_l2(const void* p) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// per-thread asynchronous global -> shared copies (16 or 8 bytes), tracked in
+// this thread's cp.async groups
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* dst_smem, const void* src) {
+  static_assert(BYTES == 16 || BYTES == 8, "cp.async size");
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst_smem)), "l"(src)
+                 : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_u32(dst_smem)), "l"(src)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// all but the newest `N` of this thread's cp.async groups have completed
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
