@@ -192,10 +192,13 @@ SC_API int32_t sc_sample_static(const void* d_state, int32_t n_qubits, int32_t d
                                 int32_t* d_outcomes, void* stream);
 
 /* ---- host-only planner inspection (no GPU needed; used by the test suite) --- */
-/* Op indices in the order the fused sweeps apply them; returns the gate count. */
+/* Op indices in the order the fused sweeps apply them; returns the gate count.
+ * Also reports the number of sweeps, stages, sweeps that change the qubit layout
+ * and layout-restoring permutation passes (any out pointer may be NULL). */
 SC_API int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
                             int32_t low_qubits, int32_t nr, double budget, int64_t* order,
-                            int64_t* n_sweeps, int64_t* n_stages);
+                            int64_t* n_sweeps, int64_t* n_stages, int64_t* n_relayouts,
+                            int64_t* n_restores);
 /* Executes the sweep plan on a host complex128 state (interleaved doubles) with the
  * kernel's tile / stage / register semantics; returns the number of sweeps. */
 SC_API int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,

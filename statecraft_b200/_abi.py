@@ -125,6 +125,7 @@ SIGNATURES = {
     "sc_debug_plan_order": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_double, _P(ctypes.c_int64),
+                                             _P(ctypes.c_int64), _P(ctypes.c_int64),
                                              _P(ctypes.c_int64), _P(ctypes.c_int64)]),
     "sc_debug_emulate_sweeps": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                                  ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,

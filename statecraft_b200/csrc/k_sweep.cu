@@ -239,11 +239,22 @@ __device__ __forceinline__ uint32_t stage_l0(uint32_t tid, const SwStage& s) {
   return x;
 }
 
+// tile position bits -> physical offset in the output layout
+template <typename P>
+__device__ __forceinline__ uint32_t spread_out32(uint32_t x, const P& p) {
+  uint32_t g = 0;
+#pragma unroll 1
+  for (int k = 0; x; ++k, x >>= 1)
+    if (x & 1u) g |= 1u << p.outp[k];
+  return g;
+}
+
+// physical offset of tile t: its index bits spread over the non-tile bits
 template <typename P>
 __device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
   uint32_t base = t << p.L;
 #pragma unroll 1
-  for (int k = 0; k < p.h; ++k) base = insert_zero32(base, p.hq[k]);
+  for (int k = 0; k < p.h; ++k) base = insert_zero32(base, p.hs[k]);
   return base;
 }
 
@@ -331,7 +342,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   const uint32_t l0_first = stage_l0<NR>(tid, p.stages[0]);
   const uint32_t l0_last = stage_l0<NR>(tid, p.stages[ns - 1]);
   const uint32_t gt_first = kTma ? 0u : spread32(l0_first, p);
-  const uint32_t gt_last = kTma ? 0u : spread32(l0_last, p);
+  const uint32_t gt_last = kTma ? 0u : spread_out32(l0_last, p);
 
   // direct path: each thread copies the amplitudes of its own first-stage registers
   // of the next tile into the other buffer with cp.async while this tile computes
@@ -590,7 +601,9 @@ template <typename R, int NR>
 cudaError_t launch_pick(void* state, const SweepParams<R>& p, int* err, int sm_count,
                         cudaStream_t s) {
   const uint32_t seg_bytes = (uint32_t)sizeof(typename Amp<R>::type) << p.L;
-  if (seg_bytes >= kTmaMinSegmentBytes) return launch_nr<R, NR, true>(state, p, err, sm_count, s);
+  // the bulk-copy store writes segments back where they came from: no relayout
+  if (seg_bytes >= kTmaMinSegmentBytes && !p.relayout)
+    return launch_nr<R, NR, true>(state, p, err, sm_count, s);
   return launch_nr<R, NR, false>(state, p, err, sm_count, s);
 }
 
@@ -614,6 +627,13 @@ uint32_t host_spread(uint32_t x, const SwSweep& sw) {
   return g;
 }
 
+uint32_t host_spread_out(uint32_t x, const SwSweep& sw) {
+  uint32_t g = 0;
+  for (int k = 0; x; ++k, x >>= 1)
+    if (x & 1u) g |= 1u << sw.outp[k];
+  return g;
+}
+
 uint32_t host_swz(uint32_t i, int shift) { return i ^ ((i >> shift) & ((1u << shift) - 1u)); }
 
 // Copies sweep `k` of `plan` into the kernel-parameter form (sweep-local indices,
@@ -630,9 +650,13 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
   p->h = sw.h;
   p->nr = sw.nr;
   p->n_stages = ns;
-  p->pad = 0;
+  p->relayout = sw.relayout;
   p->tiles = sw.tiles;
-  for (int q = 0; q < SW_MAX_HIGH; ++q) p->hq[q] = sw.hq[q];
+  for (int q = 0; q < SW_MAX_HIGH; ++q) {
+    p->hq[q] = sw.hq[q];
+    p->hs[q] = sw.hs[q];
+  }
+  for (int q = 0; q < 32; ++q) p->outp[q] = (uint8_t)sw.outp[q];
   const int shift = Amp<R>::kSwizzleShift;
   const int nv = 1 << sw.nr;
   for (int s = 0; s < ns; ++s) {
@@ -659,7 +683,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
     const int pj = (j < nv) ? last.perm[j] : j;
     p->gfirst[j] = host_spread(p->tabs[0].off[j], sw);
     p->lastoff[j] = p->tabs[ns - 1].off[pj];
-    p->glast[j] = host_spread(p->lastoff[j], sw);
+    p->glast[j] = host_spread_out(p->lastoff[j], sw);
   }
   const int32_t pool_lo = (g_hi > g_lo) ? plan.gates[g_lo].moff : 0;
   for (int g = g_lo; g < g_hi; ++g) {

@@ -212,6 +212,53 @@ bool is_parity_diag(const PGate& g) {
   return g.m[0] == g.m[6] && g.m[1] == g.m[7] && g.m[2] == g.m[4] && g.m[3] == g.m[5];
 }
 
+// In-place bit permutations that take the layout phys_of back to the identity:
+// transpositions of physical bits, grouped while their bits (plus the low bits,
+// which keep the copies coalesced) fit one permutation tile.
+std::vector<SwPerm> restore_identity(const int* phys_in, int n) {
+  int phys_of[64], log_of[64];
+  for (int q = 0; q < n; ++q) {
+    phys_of[q] = phys_in[q];
+    log_of[phys_in[q]] = q;
+  }
+  std::vector<std::pair<int, int>> swaps;
+  for (int q = 0; q < n; ++q) {
+    const int b = phys_of[q];
+    if (b == q) continue;
+    const int r = log_of[q];  // the qubit on bit q moves to bit b
+    swaps.emplace_back(q, b);
+    phys_of[q] = q; log_of[q] = q;
+    phys_of[r] = b; log_of[b] = r;
+  }
+  std::vector<SwPerm> out;
+  const int base_bits = std::min(n, 4);
+  size_t i = 0;
+  while (i < swaps.size()) {
+    uint64_t S = (base_bits >= 64) ? ~0ULL : ((1ULL << base_bits) - 1ULL);
+    int cur[64];
+    for (int b = 0; b < 64; ++b) cur[b] = b;
+    size_t j = i;
+    for (; j < swaps.size(); ++j) {
+      const uint64_t S2 = S | (1ULL << swaps[j].first) | (1ULL << swaps[j].second);
+      if (popc(S2) > SW_PERM_MAX_BITS) break;
+      S = S2;
+      std::swap(cur[swaps[j].first], cur[swaps[j].second]);
+    }
+    SwPerm pm;
+    std::memset(&pm, 0, sizeof pm);
+    int idx[64];
+    for (uint64_t m = S; m; m &= m - 1) {
+      const int b = __builtin_ctzll(m);
+      idx[b] = pm.nbits;
+      pm.bits[pm.nbits++] = (int8_t)b;
+    }
+    for (int k = 0; k < pm.nbits; ++k) pm.src[k] = (int8_t)idx[cur[pm.bits[k]]];
+    out.push_back(pm);
+    i = j;
+  }
+  return out;
+}
+
 }  // namespace
 
 Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
@@ -230,8 +277,14 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
   T = std::max(T, std::min(n, std::max(NR, L0 + 2)));
   const int L = std::min(L0, T);
   const int h = T - L;
-  const uint64_t low_qmask = (L >= 64) ? ~0ULL : ((1ULL << L) - 1ULL);
   const bool high_edges = h >= NR;  // first/last stage can use only high positions
+  // qubit layout (logical <-> physical), identity at the start and the end
+  int phys_of[64], log_of[64];
+  for (int q = 0; q < 64; ++q) phys_of[q] = log_of[q] = q;
+  const bool use_relayout = pp.relayout && high_edges && L >= 1 && n > T;
+  // unscheduled gates the relayout lookahead inspects
+  const int kLookahead = 8 * T;
+  constexpr int kNever = 1 << 30;
 
   Dag dag = build_dag(gates, n);
   std::vector<int32_t> when(G, -1);
@@ -242,6 +295,9 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
   std::vector<char> staged;
 
   while (first < G) {
+    // logical qubits on the contiguous low physical bits: free for this sweep
+    uint64_t low_qmask = 0;
+    for (int p = 0; p < L; ++p) low_qmask |= 1ULL << log_of[p];
     uint64_t H = 0;
     int hcount = 0;
     double used = 0.0;
@@ -267,27 +323,137 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       when[g] = sweep_id;
       list.push_back(g);
     }
-    // pad the high set to exactly h qubits so every sweep tile has 2^T amplitudes
-    for (int q = L; q < n && hcount < h; ++q)
-      if (!((H >> q) & 1ULL)) { H |= 1ULL << q; ++hcount; }
+    // lookahead: rank of the first later gate that needs each qubit in a tile
+    int first_need[64];
+    for (int q = 0; q < 64; ++q) first_need[q] = kNever;
+    bool more = false;
+    {
+      int seen = 0;
+      for (int g = first; g < G && seen < kLookahead; ++g) {
+        if (when[g] >= 0) continue;
+        more = true;
+        ++seen;
+        for (uint64_t m = dense_mask(gates[g]); m; m &= m - 1) {
+          const int q = __builtin_ctzll(m);
+          if (first_need[q] == kNever) first_need[q] = seen;
+        }
+      }
+      for (int g = first; g < G && !more; ++g) more = when[g] < 0;
+    }
+    // pad the high set to exactly h qubits so every sweep tile has 2^T amplitudes;
+    // qubits needed soonest first, so a relayout can bring them low
+    if (hcount < h) {
+      std::vector<int> cand;
+      for (int q = 0; q < n; ++q)
+        if (!((low_qmask >> q) & 1ULL) && !((H >> q) & 1ULL)) cand.push_back(q);
+      // ties: qubits away from their home bit first (a chance to send them home)
+      std::stable_sort(cand.begin(), cand.end(), [&](int a, int b) {
+        if (first_need[a] != first_need[b]) return first_need[a] < first_need[b];
+        const bool ma = phys_of[a] != a, mb = phys_of[b] != b;
+        if (ma != mb) return ma;
+        return phys_of[a] < phys_of[b];
+      });
+      for (size_t k = 0; k < cand.size() && hcount < h; ++k) {
+        H |= 1ULL << cand[k];
+        ++hcount;
+      }
+    }
+
+    // relayout: swap up to NR high qubits needed soon with low qubits needed later
+    // (after the last gates: the qubits whose home is low come back)
+    std::vector<int> incoming, outgoing;
+    if (use_relayout) {
+      auto need_rank = [&](int q) {
+        if (more) return first_need[q];
+        return q < L ? 0 : kNever;
+      };
+      std::vector<int> in_c, out_c;
+      for (uint64_t m = H; m; m &= m - 1) in_c.push_back(__builtin_ctzll(m));
+      for (int p = 0; p < L; ++p) out_c.push_back(log_of[p]);
+      std::stable_sort(in_c.begin(), in_c.end(),
+                       [&](int a, int b) { return need_rank(a) < need_rank(b); });
+      std::stable_sort(out_c.begin(), out_c.end(),
+                       [&](int a, int b) { return need_rank(a) > need_rank(b); });
+      for (size_t k = 0; k < in_c.size() && k < out_c.size() && (int)k < NR; ++k) {
+        if (need_rank(in_c[k]) >= need_rank(out_c[k])) break;
+        incoming.push_back(in_c[k]);
+        outgoing.push_back(out_c[k]);
+      }
+    }
+    const int n_in = (int)incoming.size();
 
     SwSweep sw;
     std::memset(&sw, 0, sizeof sw);
     sw.T = T; sw.L = L; sw.h = h; sw.nr = NR;
     sw.tiles = 1LL << (n - T);
     int pos_of[64];
+    int log_at[32];  // logical qubit at each tile position
     for (int q = 0; q < 64; ++q) pos_of[q] = -1;
-    for (int q = 0; q < L; ++q) pos_of[q] = q;
+    for (int p = 0; p < L; ++p) {
+      pos_of[log_of[p]] = p;
+      log_at[p] = log_of[p];
+    }
     {
-      int k = 0;
+      // incoming qubits take the first high positions, the rest follow by physical bit
+      std::vector<int> order(incoming.begin(), incoming.end());
+      std::sort(order.begin(), order.end(),
+                [&](int a, int b) { return phys_of[a] < phys_of[b]; });
+      std::vector<int> rest;
       for (uint64_t m = H; m; m &= m - 1) {
         const int q = __builtin_ctzll(m);
-        sw.hq[k] = q;
-        pos_of[q] = L + k;
-        ++k;
+        if (std::find(incoming.begin(), incoming.end(), q) == incoming.end()) rest.push_back(q);
+      }
+      std::sort(rest.begin(), rest.end(), [&](int a, int b) { return phys_of[a] < phys_of[b]; });
+      order.insert(order.end(), rest.begin(), rest.end());
+      for (int k = 0; k < h; ++k) {
+        sw.hq[k] = phys_of[order[k]];
+        sw.hs[k] = sw.hq[k];
+        pos_of[order[k]] = L + k;
+        log_at[L + k] = order[k];
+      }
+      std::sort(sw.hs, sw.hs + h);
+    }
+    // output layout: staying low qubits, then incoming ones, on the low physical bits;
+    // every other tile qubit goes to its home bit when that bit is in the tile
+    uint32_t out_pos = 0;  // positions of the outgoing qubits
+    for (int q : outgoing) out_pos |= 1u << pos_of[q];
+    {
+      int next_low = 0;
+      for (int p = 0; p < L; ++p)
+        if (!((out_pos >> p) & 1u)) sw.outp[p] = (int8_t)next_low++;
+      for (int k = 0; k < n_in; ++k) sw.outp[L + k] = (int8_t)next_low++;
+      std::vector<char> taken(64, 0);
+      std::vector<int> rest_pos;
+      for (int p = 0; p < T; ++p) {
+        const bool low_dest = (p < L && !((out_pos >> p) & 1u)) || (p >= L && p < L + n_in);
+        if (!low_dest) rest_pos.push_back(p);
+      }
+      // the low bits all went to staying / incoming qubits: the rest share the high bits
+      std::vector<int> avail(sw.hq, sw.hq + h);
+      std::vector<char> done(32, 0);
+      for (int p : rest_pos) {
+        const int home = log_at[p];
+        if (home >= L && std::find(avail.begin(), avail.end(), home) != avail.end() && !taken[home]) {
+          sw.outp[p] = (int8_t)home;
+          taken[home] = 1;
+          done[p] = 1;
+        }
+      }
+      std::sort(avail.begin(), avail.end());
+      size_t ai = 0;
+      for (int p : rest_pos) {
+        if (done[p]) continue;
+        while (taken[avail[ai]]) ++ai;
+        sw.outp[p] = (int8_t)avail[ai];
+        taken[avail[ai]] = 1;
       }
     }
+    for (int p = 0; p < T; ++p) {
+      const int in_phys = p < L ? p : sw.hq[p - L];
+      if (sw.outp[p] != in_phys) sw.relayout = 1;
+    }
     const uint32_t high_pos = (T >= 32 ? 0xFFFFFFFFu : ((1u << T) - 1u)) & ~((1u << L) - 1u);
+    const uint32_t in_pos = ((1u << n_in) - 1u) << L;  // positions of the incoming qubits
     const uint64_t tile_qmask = low_qmask | H;
 
     // ---- stages -----------------------------------------------------------
@@ -370,13 +536,30 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       remaining -= sg.size();
       stage_list.emplace_back(R, std::move(sg));
     }
-    // a last stage that needs low positions gets a trailing empty high stage
-    if (high_edges && (stage_list.back().first & ~high_pos))
-      stage_list.emplace_back(0u, std::vector<int32_t>());
+    // The last stage's lanes must walk the positions that land on the low physical
+    // bits: without a low swap those are positions 0..L-1 (registers high only);
+    // with one, registers hold exactly the outgoing low positions plus high ones
+    // past the incoming positions.  Otherwise a trailing empty stage does the store.
+    {
+      const uint32_t Rl = stage_list.back().first;
+      const bool single = stage_list.size() == 1;
+      bool fits;
+      if (n_in == 0)
+        fits = !high_edges || !(Rl & ~high_pos);
+      else
+        fits = !single && !(Rl & ~high_pos & ~out_pos) && !(Rl & in_pos) &&
+               popc(Rl | out_pos) <= NR;
+      if (!fits) stage_list.emplace_back(0u, std::vector<int32_t>());
+    }
 
     for (size_t s = 0; s < stage_list.size(); ++s) {
       uint32_t R = stage_list[s].first;
-      const bool edge = (s == 0) || (s + 1 == stage_list.size());
+      const bool is_last = s + 1 == stage_list.size();
+      const bool edge = (s == 0) || is_last;
+      if (is_last && n_in > 0) {
+        R |= out_pos;
+        for (int p = L + n_in; p < T && popc(R) < NR; ++p) R |= 1u << p;
+      }
       // pad R to NR positions: high positions on the edges, low ones elsewhere
       if (edge && high_edges) {
         for (int p = L; p < T && popc(R) < NR; ++p) R |= 1u << p;
@@ -466,9 +649,9 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         for (uint64_t m = pg.cmask; m; m &= m - 1) {
           const int c = __builtin_ctzll(m);
           if (pos_of[c] >= 0) sg.lmask |= 1u << pos_of[c];
-          else sg.gmask |= 1ULL << c;
+          else sg.gmask |= 1ULL << phys_of[c];
         }
-        auto ref = [&](int q) { return pos_of[q] >= 0 ? pos_of[q] : -q - 1; };
+        auto ref = [&](int q) { return pos_of[q] >= 0 ? pos_of[q] : -phys_of[q] - 1; };
         sg.moff = (int32_t)plan.pool.size();
         switch (pg.kind) {
           case PK_DENSE1:
@@ -545,11 +728,18 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     }
     sw.s1 = (int32_t)plan.stages.size();
     plan.sweeps.push_back(sw);
+    // the layout after this sweep
+    for (int p = 0; p < T; ++p) {
+      const int q = log_at[p];
+      phys_of[q] = sw.outp[p];
+      log_of[sw.outp[p]] = q;
+    }
 
     for (int32_t g : list) idx_in_sweep[g] = -1;
     ++sweep_id;
     while (first < G && when[first] >= 0) ++first;
   }
+  plan.restore = restore_identity(phys_of, n);
   return plan;
 }
 

@@ -38,7 +38,7 @@ int fail_cuda(cudaError_t e, const char* where) {
 const char* kernel_class_name(int cls) {
   static const char* names[KC_COUNT] = {"sweep",  "gate_dense", "gate_perm", "gate_diag",
                                         "init",   "probabilities", "sample",  "noise",
-                                        "expect", "adjoint",    "batch"};
+                                        "expect", "adjoint",    "batch",   "permute"};
   return (cls >= 0 && cls < KC_COUNT) ? names[cls] : "unknown";
 }
 
@@ -240,6 +240,7 @@ PlanParams Ctx::plan_params() const {
                                    : (cfg.sweep_budget < 0 ? -1.0 : (c64 ? 160.0 : 96.0));
   pp.max_gates = kSweepMaxGates;
   pp.max_pool = kSweepMaxPool;
+  pp.relayout = relayout;
   return pp;
 }
 
@@ -268,6 +269,12 @@ int Ctx::apply_gates(const std::vector<PGate>& gates) {
                                  sm_count, stream);
     mark_end();
     if (e != cudaSuccess) return fail_cuda(e, "sweep kernel");
+  }
+  for (const SwPerm& pm : plan.restore) {
+    mark_begin(KC_PERMUTE, 2.0 * dim * amp_bytes);
+    cudaError_t e = launch_permute(cfg.dtype, state.p, n, pm, sm_count, stream);
+    mark_end();
+    if (e != cudaSuccess) return fail_cuda(e, "layout restore kernel");
   }
   plan_sweeps_count += (int64_t)plan.sweeps.size();
   plan_gates += plan.n_gates;
@@ -446,6 +453,7 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
   }
   if (const char* v = getenv("STATECRAFT_B200_LOW_QUBITS")) c->low_qubits = atoi(v);
   if (const char* v = getenv("STATECRAFT_B200_NR")) c->nr = atoi(v);
+  if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) c->relayout = atoi(v) != 0;
   *out_ctx = c;
   return SC_OK;
 }

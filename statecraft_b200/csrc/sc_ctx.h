@@ -30,6 +30,7 @@ struct Ctx {
   int max_qubits = SC_DEFAULT_MAX_QUBITS;
   int low_qubits = 0;  // planner overrides (0 = default)
   int nr = 0;
+  bool relayout = true;
 
   // state
   int n = 0;

@@ -7,6 +7,7 @@
 // 2^NR amplitudes straight from the state).  Tests use both to check the planner
 // and the plan encoding on CPU.
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -25,6 +26,7 @@ PlanParams debug_params(int tile, int low, int nr, double budget) {
   pp.budget = budget;
   pp.max_gates = kSweepMaxGates;
   pp.max_pool = kSweepMaxPool;
+  if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) pp.relayout = atoi(v) != 0;
   return pp;
 }
 
@@ -43,11 +45,18 @@ int normalise_all(int n, const sc_op* ops, int64_t n_ops, std::vector<PGate>& ou
   return SC_OK;
 }
 
-inline uint64_t spread_h(uint32_t x, const SwSweep& sw) {
+inline uint64_t spread_in(uint32_t x, const SwSweep& sw) {
   uint64_t g = x & ((1u << sw.L) - 1u);
   uint32_t hi = x >> sw.L;
   for (int k = 0; hi; ++k, hi >>= 1)
     if (hi & 1u) g |= 1ULL << sw.hq[k];
+  return g;
+}
+
+inline uint64_t spread_out(uint32_t x, const SwSweep& sw) {
+  uint64_t g = 0;
+  for (int p = 0; x; ++p, x >>= 1)
+    if (x & 1u) g |= 1ULL << sw.outp[p];
   return g;
 }
 
@@ -64,18 +73,29 @@ inline C mac2(const double* m0, C a0, const double* m1, C a1) {
           m0[0] * a0.i + m0[1] * a0.r + m1[0] * a1.i + m1[1] * a1.r};
 }
 
+// One sweep: every tile is gathered through the input layout into a buffer indexed
+// by tile position, the stages run on it (register j of a thread leaves the stage
+// at position l0 | off[perm[j]]), and the tile is scattered through the output
+// layout -- the kernel's shared-memory tile, exchanges and final store.
 void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
   const int NR = sw.nr, NV = 1 << NR;
+  const uint32_t tsize = 1u << sw.T;
   const uint32_t threads = 1u << (sw.T - NR);
-  std::vector<C> v(NV);
+  std::vector<C> tb(tsize), v(NV);
+  std::vector<uint64_t> in_addr(tsize), out_addr(tsize);
+  for (uint32_t e = 0; e < tsize; ++e) {
+    in_addr[e] = spread_in(e, sw);
+    out_addr[e] = spread_out(e, sw);
+  }
   std::vector<uint32_t> off(NV);
-  std::vector<uint64_t> gidx(NV), out(NV);
   for (int64_t t = 0; t < sw.tiles; ++t) {
     uint64_t base = (uint64_t)t << sw.L;
     for (int k = 0; k < sw.h; ++k) {
-      const int b = sw.hq[k];
+      const int b = sw.hs[k];
       base = ((base >> b) << (b + 1)) | (base & ((1ULL << b) - 1ULL));
     }
+    for (uint32_t e = 0; e < tsize; ++e)
+      tb[e] = {st[2 * (base | in_addr[e])], st[2 * (base | in_addr[e]) + 1]};
     for (int s = sw.s0; s < sw.s1; ++s) {
       const SwStage& stg = plan.stages[s];
       for (uint32_t tid = 0; tid < threads; ++tid) {
@@ -89,8 +109,7 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
           for (int k = 0; k < NR; ++k)
             if (j & (1 << k)) o |= 1u << stg.R[k];
           off[j] = o;
-          gidx[j] = base | spread_h(l0 | o, sw);
-          v[j] = {st[2 * gidx[j]], st[2 * gidx[j] + 1]};
+          v[j] = tb[l0 | o];
         }
         for (int gi = stg.g0; gi < stg.g1; ++gi) {
           const SwGate& g = plan.gates[gi];
@@ -202,15 +221,42 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
           }
         }
         // folded permutations: register j leaves the stage as register perm[j]
-        for (int j = 0; j < NV; ++j) {
-          const uint64_t dst = gidx[stg.perm[j]];
-          out[j] = dst;
-        }
-        for (int j = 0; j < NV; ++j) {
-          st[2 * out[j]] = v[j].r;
-          st[2 * out[j] + 1] = v[j].i;
-        }
+        for (int j = 0; j < NV; ++j) tb[l0 | off[stg.perm[j]]] = v[j];
       }
+    }
+    for (uint32_t e = 0; e < tsize; ++e) {
+      st[2 * (base | out_addr[e])] = tb[e].r;
+      st[2 * (base | out_addr[e]) + 1] = tb[e].i;
+    }
+  }
+}
+
+// In-place permutation of physical qubit bits (launch_permute semantics).
+void emulate_permute(double* st, int n, const SwPerm& pm) {
+  const uint32_t tsize = 1u << pm.nbits;
+  std::vector<C> tb(tsize);
+  std::vector<uint64_t> addr(tsize);
+  for (uint32_t e = 0; e < tsize; ++e) {
+    uint64_t g = 0;
+    for (int k = 0; k < pm.nbits; ++k)
+      if ((e >> k) & 1u) g |= 1ULL << pm.bits[k];
+    addr[e] = g;
+  }
+  const int64_t tiles = 1LL << (n - pm.nbits);
+  for (int64_t t = 0; t < tiles; ++t) {
+    uint64_t base = (uint64_t)t;
+    for (int k = 0; k < pm.nbits; ++k) {
+      const int b = pm.bits[k];
+      base = ((base >> b) << (b + 1)) | (base & ((1ULL << b) - 1ULL));
+    }
+    for (uint32_t e = 0; e < tsize; ++e)
+      tb[e] = {st[2 * (base | addr[e])], st[2 * (base | addr[e]) + 1]};
+    for (uint32_t o = 0; o < tsize; ++o) {
+      uint32_t i = 0;
+      for (int k = 0; k < pm.nbits; ++k)
+        if ((o >> k) & 1u) i |= 1u << pm.src[k];
+      st[2 * (base | addr[o])] = tb[i].r;
+      st[2 * (base | addr[o]) + 1] = tb[i].i;
     }
   }
 }
@@ -221,7 +267,8 @@ extern "C" {
 
 int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
                             int32_t low_qubits, int32_t nr, double budget, int64_t* order,
-                            int64_t* n_sweeps, int64_t* n_stages) {
+                            int64_t* n_sweeps, int64_t* n_stages, int64_t* n_relayouts,
+                            int64_t* n_restores) {
   std::vector<PGate> gates;
   int rc = normalise_all(n, ops, n_ops, gates);
   if (rc != SC_OK) return rc;
@@ -231,6 +278,11 @@ int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, int32_t 
     for (size_t i = 0; i < plan.gate_ops.size(); ++i) order[i] = plan.gate_ops[i];
   if (n_sweeps) *n_sweeps = (int64_t)plan.sweeps.size();
   if (n_stages) *n_stages = (int64_t)plan.stages.size();
+  if (n_relayouts) {
+    *n_relayouts = 0;
+    for (const SwSweep& sw : plan.sweeps) *n_relayouts += sw.relayout ? 1 : 0;
+  }
+  if (n_restores) *n_restores = (int64_t)plan.restore.size();
   return (int32_t)plan.gate_ops.size();
 }
 
@@ -243,6 +295,7 @@ int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int3
   Plan plan = plan_sweeps(gates, n, debug_params(tile_qubits, low_qubits, nr, budget));
   if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
   for (const SwSweep& sw : plan.sweeps) emulate_sweep(state, plan, sw);
+  for (const SwPerm& pm : plan.restore) emulate_permute(state, n, pm);
   return (int32_t)plan.sweeps.size();
 }
 

@@ -99,11 +99,34 @@ struct SwStage {    // 32 bytes
   int8_t perm[16];
 };
 
+// Qubit layout.  The planner keeps a logical -> physical map of the qubits: the
+// amplitude of logical basis index x lives at the physical index whose bit
+// phys[q] is bit q of x.  Every sweep reads its tile through the layout in force
+// and may write it back through a new one (a "relayout"): up to NR of the tile's
+// high qubits move onto the contiguous low physical bits for the sweeps that
+// follow, the low qubits they displace take their physical bits.  A plan ends
+// with the identity layout; when the last sweep cannot restore it, `restore`
+// holds in-place bit permutations that do.
 struct SwSweep {
   int32_t T, L, h, nr;
   int32_t s0, s1;            // stage range
   int64_t tiles;
-  int32_t hq[SW_MAX_HIGH];   // ascending
+  int32_t hq[SW_MAX_HIGH];   // physical bit of tile position L + k (input layout)
+  int32_t hs[SW_MAX_HIGH];   // the same physical bits, ascending (tile enumeration)
+  int8_t outp[32];           // physical bit tile position p is written to (output layout)
+  int32_t relayout;          // outp differs from the input map
+};
+
+// In-place permutation of physical qubit bits: the tile is the 2^nbits
+// amplitudes that differ in bits[0..nbits-1] (ascending), and the content of
+// physical bit bits[src[k]] moves to physical bit bits[k] (tile element o takes
+// the amplitude of tile element sum_k bit_k(o) << src[k]).  The bit set is closed
+// under the permutation, so every tile reads and writes the same addresses.
+constexpr int SW_PERM_MAX_BITS = 12;
+struct SwPerm {
+  int32_t nbits;
+  int8_t bits[SW_PERM_MAX_BITS];
+  int8_t src[SW_PERM_MAX_BITS];
 };
 
 struct PlanParams {
@@ -113,6 +136,7 @@ struct PlanParams {
   double budget;     // FMA per amplitude per sweep; < 0 unlimited
   int max_gates;     // per sweep
   int max_pool = 1 << 30;  // matrix reals per sweep
+  bool relayout = true;    // let sweeps move qubits onto the low physical bits
 };
 
 // matrix reals a normalised gate stores in the sweep pool
@@ -124,6 +148,7 @@ struct Plan {
   std::vector<SwGate> gates;
   std::vector<double> pool;
   std::vector<int64_t> gate_ops;  // host only: op index of each entry of `gates`
+  std::vector<SwPerm> restore;    // bit permutations back to the identity layout
   int64_t n_gates = 0;
   bool ok = true;  // false if some gate could not be staged (planner invariant broken)
 };
@@ -147,6 +172,7 @@ enum KernelClass : int32_t {
   KC_EXPECT,
   KC_ADJOINT,
   KC_BATCH,
+  KC_PERMUTE,
   KC_COUNT
 };
 const char* kernel_class_name(int cls);
@@ -160,6 +186,9 @@ cudaError_t launch_gate(int dtype, void* state, int n, const PGate& g, cudaStrea
 // bulk-copy wait times out
 cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int* err,
                          int sm_count, cudaStream_t s);
+// in-place qubit-bit permutation of an n-qubit state
+cudaError_t launch_permute(int dtype, void* state, int n, const SwPerm& perm, int sm_count,
+                           cudaStream_t s);
 // |0..0> or |basis>
 cudaError_t launch_init_basis(int dtype, void* state, int n, uint64_t basis, cudaStream_t s);
 // c128 host layout -> device amplitudes (dtype conversion for c64)

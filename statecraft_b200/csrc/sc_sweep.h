@@ -25,9 +25,11 @@ struct SwStageTab {
 template <typename R>
 struct SweepParams {
   int32_t T, L, h, nr;
-  int32_t n_stages, pad;
+  int32_t n_stages, relayout;
   int64_t tiles;
-  int32_t hq[SW_MAX_HIGH];
+  int32_t hq[SW_MAX_HIGH];  // physical bit of tile position L + k (input layout)
+  int32_t hs[SW_MAX_HIGH];  // the same bits ascending (tile enumeration)
+  uint8_t outp[32];         // physical bit of tile position p in the output layout
   uint32_t gfirst[16];   // global offset of register j in the first stage's layout
   uint32_t glast[16];    // global offset register j is stored to (last stage, perm applied)
   uint16_t lastoff[16];  // tile offset register j is stored to (last stage, perm applied)

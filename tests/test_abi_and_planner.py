@@ -56,16 +56,21 @@ def test_invalid_handle_rejected():
     assert lib.sc_destroy(None) == A.SC_OK
 
 
-def _plan_order(c, tile, low, nr, budget):
+def _plan_info(c, tile, low, nr, budget):
     ops, n_ops = serialize_circuit(c)
     order = np.zeros(max(1, n_ops), dtype=np.int64)
-    sweeps = ctypes.c_int64()
-    stages = ctypes.c_int64()
+    cnt = [ctypes.c_int64() for _ in range(4)]
     k = A.load().sc_debug_plan_order(c.qubitCount, ops, n_ops, tile, low, nr, budget,
                                      order.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
-                                     ctypes.byref(sweeps), ctypes.byref(stages))
+                                     *[ctypes.byref(x) for x in cnt])
     assert k >= 0
-    return order[:k], sweeps.value, stages.value
+    sweeps, stages, relayouts, restores = (x.value for x in cnt)
+    return order[:k], dict(sweeps=sweeps, stages=stages, relayouts=relayouts, restores=restores)
+
+
+def _plan_order(c, tile, low, nr, budget):
+    order, info = _plan_info(c, tile, low, nr, budget)
+    return order, info["sweeps"], info["stages"]
 
 
 def _emulate(c, state, tile, low, nr, budget):
@@ -140,3 +145,34 @@ def test_brickwall_plan_uses_few_sweeps():
     order, sweeps, stages = _plan_order(c, 11, 4, 3, -1.0)
     assert len(order) == len(c.operations)
     assert sweeps <= 3 * 20  # unfused would be 590 sweeps
+
+
+@pytest.mark.parametrize("n,layers,cfg", [
+    (16, 12, (8, 3, 3, -1.0)),
+    (16, 12, (8, 4, 3, 40.0)),
+    (17, 10, (9, 2, 2, -1.0)),
+    (18, 8, (10, 4, 3, -1.0)),
+])
+def test_relayout_plans_match_oracle(n, layers, cfg):
+    # brick-wall circuits move their working window along the chain: the planner
+    # brings the next window's qubits onto the low physical bits between sweeps and
+    # restores the identity layout at the end
+    from statecraft_b200 import workloads as W
+
+    c = W.brickwall_circuit(n, layers, seed=77 + n, mcz=False, rzz=True)
+    _, info = _plan_info(c, *cfg)
+    assert info["relayouts"] > 0
+    init = RCirc.random_state(n, n)
+    got, _ = _emulate(c, init, *cfg)
+    np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
+
+
+def test_relayout_reduces_sweeps(monkeypatch):
+    from statecraft_b200 import workloads as W
+
+    c = W.brickwall_circuit(30, 40, seed=3030, mcz=False, rzz=False)
+    _, with_layout = _plan_info(c, 10, 4, 3, -1.0)
+    monkeypatch.setenv("STATECRAFT_B200_RELAYOUT", "0")
+    _, without = _plan_info(c, 10, 4, 3, -1.0)
+    assert without["relayouts"] == 0 and without["restores"] == 0
+    assert with_layout["sweeps"] < 0.8 * without["sweeps"]
