@@ -24,6 +24,9 @@ struct PermParams {
   int64_t tiles;
   int8_t bits[SW_PERM_MAX_BITS];
   int8_t src[SW_PERM_MAX_BITS];
+  // shared-memory swizzle: tile element i sits in slot i ^ (XOR of swz[k] over the
+  // set bits k of i); swz[k] only touches the bits that select a bank group
+  uint8_t swz[SW_PERM_MAX_BITS];
 };
 
 constexpr int kPermThreads = 256;
@@ -38,10 +41,12 @@ __global__ void __launch_bounds__(kPermThreads)
   uint32_t* const addr_hi = addr_lo + 64;
   uint32_t* const src_lo = addr_hi + 64;
   uint32_t* const src_hi = src_lo + 64;
-  A* const tile = reinterpret_cast<A*>(src_hi + 64);
+  uint32_t* const swz_lo = src_hi + 64;
+  uint32_t* const swz_hi = swz_lo + 64;
+  A* const tile = reinterpret_cast<A*>(swz_hi + 64);
   const uint32_t tid = threadIdx.x;
   if (tid < 64) {
-    uint32_t alo = 0, ahi = 0, slo = 0, shi = 0;
+    uint32_t alo = 0, ahi = 0, slo = 0, shi = 0, zlo = 0, zhi = 0;
     for (int k = 0; k < p.nbits; ++k) {
       const uint32_t lo_bit = (k < 6) ? ((tid >> k) & 1u) : 0u;
       const uint32_t hi_bit = (k >= 6) ? ((tid >> (k - 6)) & 1u) : 0u;
@@ -49,13 +54,18 @@ __global__ void __launch_bounds__(kPermThreads)
       ahi |= hi_bit << p.bits[k];
       slo |= lo_bit << p.src[k];
       shi |= hi_bit << p.src[k];
+      zlo ^= lo_bit ? (uint32_t)p.swz[k] : 0u;
+      zhi ^= hi_bit ? (uint32_t)p.swz[k] : 0u;
     }
     addr_lo[tid] = alo;
     addr_hi[tid] = ahi;
     src_lo[tid] = slo;
     src_hi[tid] = shi;
+    swz_lo[tid] = zlo;
+    swz_hi[tid] = zhi;
   }
   __syncthreads();
+  auto slot = [&](uint32_t i) { return i ^ swz_lo[i & 63u] ^ swz_hi[i >> 6]; };
   const uint32_t tsize = 1u << p.nbits;
   for (int64_t t = blockIdx.x; t < p.tiles; t += gridDim.x) {
     uint64_t base = (uint64_t)t;
@@ -63,10 +73,10 @@ __global__ void __launch_bounds__(kPermThreads)
     for (int k = 0; k < p.nbits; ++k) base = insert_zero64(base, p.bits[k]);
     A* const g = st + base;
     for (uint32_t e = tid; e < tsize; e += kPermThreads)
-      tile[e] = g[addr_lo[e & 63u] | addr_hi[e >> 6]];
+      tile[slot(e)] = g[addr_lo[e & 63u] | addr_hi[e >> 6]];
     __syncthreads();
     for (uint32_t o = tid; o < tsize; o += kPermThreads)
-      g[addr_lo[o & 63u] | addr_hi[o >> 6]] = tile[src_lo[o & 63u] | src_hi[o >> 6]];
+      g[addr_lo[o & 63u] | addr_hi[o >> 6]] = tile[slot(src_lo[o & 63u] | src_hi[o >> 6])];
     __syncthreads();
   }
 }
@@ -86,15 +96,39 @@ cudaError_t launch_t(void* state, int n, const SwPerm& perm, int sm_count, cudaS
   for (int k = 0; k < SW_PERM_MAX_BITS; ++k) {
     p.bits[k] = perm.bits[k];
     p.src[k] = perm.src[k];
+    p.swz[k] = 0;
   }
-  const size_t smem = 4 * 64 * sizeof(uint32_t) + (sizeof(A) << perm.nbits);
+  // A 128-byte shared-memory row holds W = 8 (complex128) or 16 (complex64)
+  // elements; lanes that access together (W of them) differ in tile bits 0..w-1
+  // on the load and in bits src[0..w-1] on the permuted read.  Give each of those
+  // source bits at or above w a bank-group vector that completes a basis with
+  // the others, so both phases are conflict-free.
+  {
+    const int w = sizeof(A) == 16 ? 3 : 4;
+    uint32_t used = 0;  // span of the bank-group vectors assigned so far (as a set of unit bits)
+    int pending[4];
+    int np = 0;
+    for (int k = 0; k < w && k < perm.nbits; ++k) {
+      const int b = perm.src[k];
+      if (b < w) used |= 1u << b;
+      else pending[np++] = b;
+    }
+    for (int i = 0; i < np; ++i) {
+      int u = 0;
+      while (u < w && ((used >> u) & 1u)) ++u;
+      if (u >= w) break;
+      p.swz[pending[i]] = (uint8_t)(1u << u);
+      used |= 1u << u;
+    }
+  }
+  const size_t smem = 6 * 64 * sizeof(uint32_t) + (sizeof(A) << perm.nbits);
   auto kern = k_permute<R>;
   {
     std::lock_guard<std::mutex> lk(g_perm_mu);
     const int di = sizeof(R) == 4 ? 1 : 0;
     if (!g_perm_attr[di]) {
       cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)(4 * 64 * sizeof(uint32_t) +
+                                           (int)(6 * 64 * sizeof(uint32_t) +
                                                  (sizeof(A) << SW_PERM_MAX_BITS)));
       if (e != cudaSuccess) return e;
       g_perm_attr[di] = true;
