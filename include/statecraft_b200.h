@@ -159,6 +159,34 @@ SC_API int32_t sc_adjoint_forward(void* ctx, int32_t n_qubits, const sc_op* ops,
                            double* out_value);
 SC_API int32_t sc_adjoint_backward(void* ctx, double* out_grad, int64_t n_params);
 
+/* Batched QAOA ring ansatz (no counterpart in the reference engine, which runs
+ * such suites one circuit at a time through simulate(); the ansatz is
+ * app/.../AlgorithmSuiteSpecs.java:186-200, phases :283-287).  Instance i has
+ * n_qubits[i] in 2..23 qubits; its circuit is H on every qubit, then for each of
+ * the p (1..16) layers exp(-i gammas[i*p+l] Z_j Z_{j+1 mod n}) on every ring edge
+ * and RX(2 betas[i*p+l]) on every qubit; the result is <sum_j Z_j Z_{j+1 mod n}>.
+ * All instances run in one captured CUDA graph of p + 3 kernels over uneven
+ * instance sizes; dtype SC_C64 keeps amplitudes in complex64 and every table and
+ * reduction in FP64.  tune = 1 times the kernel shapes on the batch and keeps the
+ * fastest.  States of instances with more than 12 qubits live in one device arena
+ * (2^n amplitudes each); smaller ones never leave shared memory.
+ * A batch belongs to its context (freed with it at the latest). */
+SC_API int32_t sc_qaoa_batch_create(void* ctx, int32_t dtype, int64_t n_inst, const int32_t* n_qubits,
+                                    int32_t p, const double* gammas, const double* betas,
+                                    int32_t tune, void** out_batch);
+/* New angles for the next runs (same shapes; the captured graph is reused). */
+SC_API int32_t sc_qaoa_batch_set_angles(void* batch, const double* gammas, const double* betas);
+/* Enqueues one run of the whole batch (one graph launch) on the context stream. */
+SC_API int32_t sc_qaoa_batch_run(void* batch);
+/* Waits for the runs and copies <sum ZZ> (and the FP64 norms) per instance, in
+ * the caller's instance order; either pointer may be NULL. */
+SC_API int32_t sc_qaoa_batch_energies(void* batch, double* energies, double* norms);
+/* Chosen shape (register group width, CTAs per SM), its tuned time per run and
+ * the algorithmic HBM bytes per run. */
+SC_API int32_t sc_qaoa_batch_info(void* batch, int32_t* nr, int32_t* ctas_per_sm, double* tuned_ms,
+                                  double* bytes_per_run);
+SC_API int32_t sc_qaoa_batch_destroy(void* batch);
+
 /* Per-kernel-class device timing collected while cfg.timing = 1:
  * for class i in [0, cap): launches[i], milliseconds[i], bytes[i] (algorithmic
  * bytes moved).  Returns the number of classes; names via sc_kernel_class_name. */

@@ -222,3 +222,20 @@ def simulate_request(request):
         outcomes = sample(st, n, qubits, instr.shots, instr.seed if instr.seed is not None else 0)
         measurement = {"qubits": tuple(qubits), "outcomes": outcomes}
     return st, measurement, chosen
+
+
+def qaoa_ring_energy(n: int, gammas, betas) -> float:
+    """<sum_j Z_j Z_{j+1 mod n}> of the QAOA ring ansatz (H on all qubits, then per layer
+    the ring ZZ phases and RX(2 beta), AlgorithmSuiteSpecs.java:186-200), gate by gate
+    on the oracle."""
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import serialize_circuit
+
+    c = W.qaoa_circuit(n, gammas, betas)
+    ops, n_ops = serialize_circuit(c)
+    st = initial_state(n)
+    rc, _ = run(n, ops, n_ops, st)
+    if rc != 0:
+        raise RuntimeError(f"oracle run failed: {rc}")
+    z = [(1 << j) | (1 << ((j + 1) % n)) for j in range(n)]
+    return expect_pauli(st, n, [0] * n, z, [1.0] * n)

@@ -111,6 +111,19 @@ SIGNATURES = {
                                             _P(ctypes.c_double)]),
     "sc_adjoint_backward": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_double),
                                              ctypes.c_int64]),
+    "sc_qaoa_batch_create": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64,
+                                              _P(ctypes.c_int32), ctypes.c_int32,
+                                              _P(ctypes.c_double), _P(ctypes.c_double),
+                                              ctypes.c_int32, _P(ctypes.c_void_p)]),
+    "sc_qaoa_batch_set_angles": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_double),
+                                                  _P(ctypes.c_double)]),
+    "sc_qaoa_batch_run": (ctypes.c_int32, [ctypes.c_void_p]),
+    "sc_qaoa_batch_energies": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_double),
+                                                _P(ctypes.c_double)]),
+    "sc_qaoa_batch_info": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int32),
+                                            _P(ctypes.c_int32), _P(ctypes.c_double),
+                                            _P(ctypes.c_double)]),
+    "sc_qaoa_batch_destroy": (ctypes.c_int32, [ctypes.c_void_p]),
     "sc_kernel_stats": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int64),
                                          _P(ctypes.c_double), _P(ctypes.c_double),
                                          ctypes.c_int32]),

@@ -464,6 +464,8 @@ int32_t sc_destroy(void* p) {
   if (c->magic != Ctx::kMagic) return fail(SC_EINVAL, "invalid context handle");
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->stream);
+  for (void* b : c->qaoa_batches) qaoa_batch_free(b);
+  c->qaoa_batches.clear();
   c->release_all();
   for (cudaEvent_t ev : c->event_pool) cudaEventDestroy(ev);
   cudaStreamDestroy(c->stream);

@@ -14,6 +14,8 @@ namespace sc {
 
 int fail(int code, const char* fmt, ...);
 int fail_cuda(cudaError_t e, const char* where);
+// frees a QAOA batch (sc_qaoa.cpp) and its device buffers
+void qaoa_batch_free(void* batch);
 
 struct DevBuf {
   void* p = nullptr;
@@ -58,6 +60,9 @@ struct Ctx {
   std::vector<uint64_t> adj_x, adj_z;
   std::vector<double> adj_c;
   bool adj_ready = false;
+
+  // QAOA batches created on this context (freed by sc_destroy)
+  std::vector<void*> qaoa_batches;
 
   // plan statistics of the last run
   int64_t plan_sweeps_count = 0, plan_gates = 0, plan_stages = 0;

@@ -235,3 +235,32 @@ def test_expectation_matches_dense_algebra():
         want = float(np.real(np.vdot(amps, mat @ amps)))
         got = O.expect_pauli(st, n, [xm], [zm], [1.0])
         assert got == pytest.approx(want, abs=1e-13)
+
+
+def test_qaoa_ring_energy_popcount_form():
+    # The batched QAOA kernels evaluate sum_j Z_j Z_{j+1 mod n} on basis state x as
+    # n - 2 popcount(x XOR rotr_n(x)) and fold a layer's ring phases into
+    # exp(-i gamma (n - 2k)); both identities checked on the oracle.
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import serialize_circuit
+
+    n = 7
+    rng = np.random.default_rng(5)
+    st = rng.normal(size=2 << n)
+    st /= np.sqrt(np.sum(st ** 2))
+    z = [(1 << j) | (1 << ((j + 1) % n)) for j in range(n)]
+    direct = O.expect_pauli(st, n, [0] * n, z, [1.0] * n)
+    probs = st[0::2] ** 2 + st[1::2] ** 2
+    x = np.arange(1 << n)
+    rot = (x >> 1) | ((x & 1) << (n - 1))
+    k = np.array([bin(v).count("1") for v in (x ^ rot)])
+    assert abs(direct - np.sum(probs * (n - 2 * k))) < 1e-12
+    # one layer of ring phases from |+>^n equals the tabulated phase per basis state
+    g = 0.37
+    c = W.qaoa_circuit(n, [g], [0.0])
+    ops, n_ops = serialize_circuit(c)
+    s2 = O.initial_state(n)
+    assert O.run(n, ops, n_ops, s2)[0] == 0
+    amp = s2[0::2] + 1j * s2[1::2]
+    want = np.exp(-1j * g * (n - 2 * k)) / np.sqrt(2.0 ** n)
+    np.testing.assert_allclose(amp, want, rtol=0, atol=1e-14)
