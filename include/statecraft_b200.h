@@ -187,6 +187,23 @@ SC_API int32_t sc_qaoa_batch_info(void* batch, int32_t* nr, int32_t* ctas_per_sm
                                   double* bytes_per_run);
 SC_API int32_t sc_qaoa_batch_destroy(void* batch);
 
+/* Batched noisy trajectories (no counterpart in the reference engine, which runs
+ * one trajectory per simulate(); trajectory semantics StatevectorEngine.java:371-600).
+ * Runs n_traj (1..65535) copies of the circuit from |0..0> in the context's dtype;
+ * trajectory t draws its Kraus branches from SplittableRandom(noise_seed + t), one
+ * nextDouble(total) per noise record in record order, and samples `shots` outcomes
+ * of all qubits from SplittableRandom(measure_seed + t).  Every record must be a
+ * Pauli mixture (each Kraus operator a scalar times I, X, Y or Z: depolarizing,
+ * bit flip, phase flip, ...); others return SC_EUNSUPPORTED.  Records are
+ * sc_channel, sorted by after_op, e.g. one per touched qubit after each gate.
+ * Outputs (caller-owned, any may be NULL): outcomes[t*shots + k] (basis index),
+ * choices[t*n_channels + j] (chosen Kraus index), states[t * 2^(n+1) ...]
+ * (interleaved doubles of every final state; small batches only). */
+SC_API int32_t sc_trajectories(void* ctx, int32_t n_qubits, const sc_op* ops, int64_t n_ops,
+                               const sc_channel* channels, int64_t n_channels, int64_t n_traj,
+                               uint64_t noise_seed, int64_t shots, uint64_t measure_seed,
+                               int32_t* outcomes, int32_t* choices, double* states);
+
 /* Per-kernel-class device timing collected while cfg.timing = 1:
  * for class i in [0, cap): launches[i], milliseconds[i], bytes[i] (algorithmic
  * bytes moved).  Returns the number of classes; names via sc_kernel_class_name. */

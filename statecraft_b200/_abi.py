@@ -124,6 +124,11 @@ SIGNATURES = {
                                             _P(ctypes.c_int32), _P(ctypes.c_double),
                                             _P(ctypes.c_double)]),
     "sc_qaoa_batch_destroy": (ctypes.c_int32, [ctypes.c_void_p]),
+    "sc_trajectories": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int32, _P(ScOp),
+                                         ctypes.c_int64, _P(ScChannel), ctypes.c_int64,
+                                         ctypes.c_int64, ctypes.c_uint64, ctypes.c_int64,
+                                         ctypes.c_uint64, _P(ctypes.c_int32),
+                                         _P(ctypes.c_int32), _P(ctypes.c_double)]),
     "sc_kernel_stats": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int64),
                                          _P(ctypes.c_double), _P(ctypes.c_double),
                                          ctypes.c_int32]),

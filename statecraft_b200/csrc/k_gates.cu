@@ -191,6 +191,25 @@ cudaError_t launch_init_basis(int dtype, void* state, int n, uint64_t basis, cud
   return cudaGetLastError();
 }
 
+// |0..0> in each of `batch` n-qubit states stored back to back
+template <typename R>
+__global__ void k_init_batch(typename Amp<R>::type* st, uint64_t total, uint64_t dim_mask) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x)
+    st[i] = make_amp<R>((i & dim_mask) == 0 ? (R)1 : (R)0, (R)0);
+}
+
+cudaError_t launch_init_batch(int dtype, void* states, int n, int64_t batch, cudaStream_t s) {
+  const uint64_t total = (uint64_t)batch << n;
+  const int grid = grid_for((int64_t)total);
+  const uint64_t mask = (1ULL << n) - 1ULL;
+  if (dtype == SC_C64)
+    k_init_batch<float><<<grid, kThreads, 0, s>>>(static_cast<float2*>(states), total, mask);
+  else
+    k_init_batch<double><<<grid, kThreads, 0, s>>>(static_cast<double2*>(states), total, mask);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_convert_in(int dtype, void* state, const double* src, int64_t count,
                               cudaStream_t s) {
   if (dtype != SC_C64)

@@ -51,26 +51,34 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;  // valid in thread 0
 }
 
-// pass A: S[c] = sum of chunk c
+// pass A: S[c] = sum of chunk c.  A batch of states of len_per entries each,
+// stored back to back, has chunks_per chunks per state (chunk c of the whole
+// array is chunk c % chunks_per of state c / chunks_per).
 template <typename Src>
-__global__ void __launch_bounds__(kThreadsA) k_chunk_sums(Src src, uint64_t len, double* sums,
+__global__ void __launch_bounds__(kThreadsA) k_chunk_sums(Src src, uint64_t len_per,
+                                                          uint64_t chunks_per, double* sums,
                                                           uint64_t chunks) {
   __shared__ double red[kThreadsA / 32];
   for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
-    const uint64_t b = c * kChunk;
+    const uint64_t st = c / chunks_per;
+    const uint64_t b = (c - st * chunks_per) * kChunk;
+    const uint64_t off = st * len_per;
     double acc = 0.0;
     for (int k = threadIdx.x; k < kChunk; k += kThreadsA) {
       const uint64_t i = b + k;
-      if (i < len) acc += src(i);
+      if (i < len_per) acc += src(off + i);
     }
     const double s = block_sum<kThreadsA>(acc, red);
     if (threadIdx.x == 0) sums[c] = s;
   }
 }
 
-// pass B (one CTA of 1024 threads): total, scale, exclusive chunk prefixes
+// pass B (one CTA of 1024 threads per state): total, scale, exclusive chunk prefixes
 __global__ void __launch_bounds__(1024) k_chunk_scan(const double* sums, uint64_t chunks,
                                                      double* prefix, SampleScalars* out) {
+  sums += blockIdx.x * chunks;
+  prefix += blockIdx.x * chunks;
+  out += blockIdx.x;
   __shared__ double part[1024];
   __shared__ double red[32];
   const uint64_t per = (chunks + 1023) / 1024;
@@ -104,20 +112,28 @@ __global__ void __launch_bounds__(1024) k_chunk_scan(const double* sums, uint64_
   }
 }
 
-// pass C: one warp per shot
+// pass C: one warp per shot.  In a batch, shot g belongs to state g / shots_per and
+// draws the (g % shots_per)-th uniform of SplittableRandom(seed + state).
 template <typename Src>
-__global__ void __launch_bounds__(256) k_sample_shots(Src src, uint64_t len, const double* prefix,
-                                                      uint64_t chunks, const SampleScalars* sc,
+__global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
+                                                      const double* prefix_all, uint64_t chunks,
+                                                      const SampleScalars* sc,
                                                       const double* uniforms, uint64_t seed,
-                                                      int64_t shots, int32_t* out) {
+                                                      int64_t shots_per, int64_t shots_total,
+                                                      int32_t* out) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  const double scale = sc->scale;
-  for (int64_t k = warp; k < shots; k += nwarps) {
-    const double u = uniforms ? uniforms[k] : splitmix_double(seed, (uint64_t)k);
+  for (int64_t g = warp; g < shots_total; g += nwarps) {
+    const int64_t stn = g / shots_per;
+    const int64_t k = g - stn * shots_per;
+    const uint64_t off = (uint64_t)stn * len;
+    auto src = [&](uint64_t i) { return src_all(off + i); };
+    const double* prefix = prefix_all + (uint64_t)stn * chunks;
+    const double scale = sc[stn].scale;
+    const double u = uniforms ? uniforms[g] : splitmix_double(seed + (uint64_t)stn, (uint64_t)k);
     if (u >= 1.0) {
-      if (lane == 0) out[k] = (int32_t)(len - 1);
+      if (lane == 0) out[g] = (int32_t)(len - 1);
       continue;
     }
     // last chunk whose prefix is < u (prefix[0] == 0)
@@ -165,7 +181,7 @@ __global__ void __launch_bounds__(256) k_sample_shots(Src src, uint64_t len, con
     if (lane == 0) {
       uint64_t r = found;
       if (r == ~0ULL) r = min(len - 1, b + kChunk);  // rounding gap: first entry of the next chunk
-      out[k] = (int32_t)r;
+      out[g] = (int32_t)r;
     }
   }
 }
@@ -251,15 +267,18 @@ cudaError_t marginal_t(const void* state, int n, uint64_t mmask, int m, double* 
 }
 
 template <typename Src>
-cudaError_t sample_src(Src src, uint64_t len, const SampleArgs& a, cudaStream_t s) {
+cudaError_t sample_src(Src src, uint64_t len, int64_t batch, const SampleArgs& a,
+                       cudaStream_t s) {
   const uint64_t chunks = (len + kChunk - 1) / kChunk;
-  k_chunk_sums<Src><<<grid_cap(chunks * kThreadsA, kThreadsA, a.sm_count), kThreadsA, 0, s>>>(
-      src, len, a.chunk_sums, chunks);
-  k_chunk_scan<<<1, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix, a.scalars);
+  const uint64_t all_chunks = chunks * (uint64_t)batch;
+  k_chunk_sums<Src><<<grid_cap(all_chunks * kThreadsA, kThreadsA, a.sm_count), kThreadsA, 0, s>>>(
+      src, len, chunks, a.chunk_sums, all_chunks);
+  k_chunk_scan<<<(unsigned)batch, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix, a.scalars);
   if (a.shots > 0) {
-    const int blocks = grid_cap((uint64_t)a.shots * 32, 256, a.sm_count);
+    const int64_t total = a.shots * batch;
+    const int blocks = grid_cap((uint64_t)total * 32, 256, a.sm_count);
     k_sample_shots<Src><<<blocks, 256, 0, s>>>(src, len, a.chunk_prefix, chunks, a.scalars,
-                                               a.uniforms, a.seed, a.shots, a.outcomes);
+                                               a.uniforms, a.seed, a.shots, total, a.outcomes);
   }
   return cudaGetLastError();
 }
@@ -276,10 +295,18 @@ cudaError_t launch_marginal(int dtype, const void* state, int n, uint64_t mmask,
 
 cudaError_t launch_sample(int dtype, const void* state, const double* probs, uint64_t len,
                           const SampleArgs& a, cudaStream_t s) {
-  if (probs) return sample_src(ArraySrc{probs}, len, a, s);
+  if (probs) return sample_src(ArraySrc{probs}, len, 1, a, s);
   if (dtype == SC_C64)
-    return sample_src(DirectSrc<float>{static_cast<const float2*>(state)}, len, a, s);
-  return sample_src(DirectSrc<double>{static_cast<const double2*>(state)}, len, a, s);
+    return sample_src(DirectSrc<float>{static_cast<const float2*>(state)}, len, 1, a, s);
+  return sample_src(DirectSrc<double>{static_cast<const double2*>(state)}, len, 1, a, s);
+}
+
+cudaError_t launch_sample_batch(int dtype, const void* states, uint64_t len, int64_t batch,
+                                const SampleArgs& a, cudaStream_t s) {
+  if (batch < 1 || batch > 65535) return cudaErrorInvalidValue;
+  if (dtype == SC_C64)
+    return sample_src(DirectSrc<float>{static_cast<const float2*>(states)}, len, batch, a, s);
+  return sample_src(DirectSrc<double>{static_cast<const double2*>(states)}, len, batch, a, s);
 }
 
 uint64_t sample_chunks(uint64_t len) { return (len + kChunk - 1) / kChunk; }

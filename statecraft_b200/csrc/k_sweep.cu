@@ -199,6 +199,29 @@ __device__ __forceinline__ void d1r(typename Amp<R>::type (&v)[1 << NR], const R
     v[j] = ((j >> A_) & 1) ? cmul(d1r_, d1i_, v[j]) : cmul(d0r, d0i, v[j]);
 }
 
+// Pauli chosen per trajectory on register bit A_: 1 = X, 2 = Y, 3 = Z (the
+// identity never reaches here)
+template <typename R, int NR, int A_>
+__device__ __forceinline__ void pauli(typename Amp<R>::type (&v)[1 << NR], uint32_t code) {
+  const bool flip = code != 3u;                  // X, Y swap the pair
+  const R s0 = code == 2u ? (R)-1 : (R)1;        // Y: new0 = -i a1, new1 = i a0
+  const R s1 = code == 1u ? (R)1 : (R)-1;        // Z: new1 = -a1
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    if (j & (1 << A_)) continue;
+    const int j1 = j | (1 << A_);
+    const auto a0 = v[j], a1 = v[j1];
+    if (code == 2u) {
+      v[j] = make_amp<R>(a1.y, s0 * a1.x);
+      v[j1] = make_amp<R>(-a0.y, a0.x);
+    } else {
+      v[j] = flip ? a1 : a0;
+      const auto b = flip ? a0 : a1;
+      v[j1] = make_amp<R>(s1 * b.x, s1 * b.y);
+    }
+  }
+}
+
 // switch cases for the dispatch code (sw_code): one jump per gate into code that
 // is specialised on its register bits
 #define SC_CASE_1(K, A, F) \
@@ -286,7 +309,9 @@ __host__ __device__ constexpr size_t sweep_smem_bytes(int T, int h, bool tma, in
 
 // kTma = true: double-buffered bulk-copy pipeline (worth it for long segments);
 // kTma = false: direct 128-/64-bit loads and stores, one exchange buffer.
-template <typename R, int NR, bool kTma>
+// kBatch = true (direct path only): the sweep runs over p.batch states back to
+// back, and Pauli slots read the trajectory's choices, staged in shared memory.
+template <typename R, int NR, bool kTma, bool kBatch>
 __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep_max_regs<R, NR>()))
     k_sweep(typename Amp<R>::type* __restrict__ st, const __grid_constant__ SweepParams<R> p,
             int* __restrict__ err) {
@@ -310,7 +335,17 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   const uint32_t seg_amps = 1u << p.L;
   const uint32_t seg_bytes = seg_amps * (uint32_t)sizeof(A);
   const uint32_t tile_bytes = tile_amps * (uint32_t)sizeof(A);
-  const uint32_t tiles = (uint32_t)p.tiles;
+  // work items: (state, tile) pairs, tile-major within a state; one state unless
+  // the sweep runs over a batch of trajectories
+  const uint32_t tiles = kBatch ? (uint32_t)(p.tiles * p.batch) : (uint32_t)p.tiles;
+  const uint32_t tile_mask = kBatch ? (uint32_t)p.tiles - 1u : 0xffffffffu;
+  auto item_state = [&](uint32_t it) -> A* {
+    if constexpr (kBatch) return st + ((uint64_t)(it >> p.tiles_log2) << p.nq);
+    return st;
+  };
+  // Pauli choices of the current trajectory for this sweep's slots
+  uint8_t* const codes = reinterpret_cast<uint8_t*>(buf1 + tile_amps);
+  uint32_t codes_for = 0xffffffffu;
 
   if constexpr (kTma) {
     // global offset of each segment (the high tile bits spread onto hq)
@@ -330,7 +365,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   }
 
   auto issue_load = [&](uint32_t t, int b) {
-    const A* src = st + tile_base(t, p);
+    const A* src = item_state(t) + tile_base(t & tile_mask, p);
     A* dst = b ? buf1 : buf0;
     if (lane == 0) mbar_arrive_expect_tx(&bars[b], tile_bytes);
     __syncwarp(pmask);
@@ -347,7 +382,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   // direct path: each thread copies the amplitudes of its own first-stage registers
   // of the next tile into the other buffer with cp.async while this tile computes
   auto prefetch_own = [&](uint32_t tt, A* dst) {
-    const A* src = st + tile_base(tt, p);
+    const A* src = item_state(tt) + tile_base(tt & tile_mask, p);
     const SwStageTab& tab0 = p.tabs[0];
 #pragma unroll
     for (int j = 0; j < NV; ++j)
@@ -390,7 +425,17 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
         break;
       }
     }
-    const uint32_t base = tile_base(t, p);
+    const uint32_t base = tile_base(t & tile_mask, p);
+    if constexpr (kBatch) {
+      const uint32_t traj = t >> p.tiles_log2;
+      if (traj != codes_for) {  // uniform: every thread of the CTA works on tile t
+        __syncthreads();       // readers of the previous trajectory's choices are done
+        for (int k = (int)tid; k < p.n_local_slots; k += (int)blockDim.x)
+          codes[k] = p.paulis[(size_t)traj * p.n_slots + p.slot_map[k]];
+        __syncthreads();
+        codes_for = traj;
+      }
+    }
 
     A v[NV];
     {
@@ -425,6 +470,10 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       for (int gi = stg.g0; gi < stg.g1; ++gi) {
         const SwGate& g = p.gates[gi];
         if (((uint64_t)base & g.gmask) != g.gmask) continue;
+        if constexpr (kBatch) {
+          // identity Pauli (the common branch): skip the record before the jump
+          if (g.kind == SK_PAULI && codes[g.b] == 0) continue;
+        }
         const R* m = p.pool + g.moff;
         const uint32_t lmask = g.lmask;
         switch (g.code) {
@@ -437,10 +486,16 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #define SC_DO_SWAP(A, B) rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v)
 #define SC_DO_X0(A) xswap0<R, NR, A>(v)
 #define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v)
+#define SC_DO_PAULI(A)                        \
+  if constexpr (kBatch) {                     \
+    pauli<R, NR, A>(v, (uint32_t)codes[g.b]); \
+  }
           SC_CASES_1(SK_X0, SC_DO_X0)
           SC_CASES_2(SK_CX0, SC_DO_CX0)
+          SC_CASES_1(SK_PAULI, SC_DO_PAULI)
 #undef SC_DO_X0
 #undef SC_DO_CX0
+#undef SC_DO_PAULI
           SC_CASES_1(SK_G1, SC_DO_G1)
           SC_CASES_1(SK_X, SC_DO_X)
           SC_CASES_1(SK_D1R, SC_DO_D1R)
@@ -536,13 +591,13 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       fence_proxy_async_smem();
       __syncthreads();
       if (producer) {
-        A* dst = st + base;
+        A* dst = item_state(t) + base;
         for (uint32_t s = lane; s < nseg; s += nprod)
           bulk_store(dst + segoff[s], cur + s * seg_amps, seg_bytes);
         bulk_commit();
       }
     } else {
-      A* __restrict__ dst = st + base;
+      A* __restrict__ dst = item_state(t) + base;
 #pragma unroll
       for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
     }
@@ -560,39 +615,39 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 
 struct LaunchCache {
   std::mutex mu;
-  bool attr_set[2][SW_MAX_NR + 1][2] = {};
+  bool attr_set[2][SW_MAX_NR + 1][2][2] = {};
 };
 LaunchCache g_cache;
 
 // Bulk copies pay off once a segment is long; shorter segments use direct loads.
 constexpr uint32_t kTmaMinSegmentBytes = 2048;
 
-template <typename R, int NR, bool kTma>
+template <typename R, int NR, bool kTma, bool kBatch>
 cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_count,
                       cudaStream_t s) {
   using A = typename Amp<R>::type;
-  auto kern = k_sweep<R, NR, kTma>;
+  auto kern = k_sweep<R, NR, kTma, kBatch>;
   const int di = std::is_same<R, float>::value ? 1 : 0;
   {
     std::lock_guard<std::mutex> lk(g_cache.mu);
-    if (!g_cache.attr_set[di][NR][kTma]) {
+    if (!g_cache.attr_set[di][NR][kTma][kBatch]) {
       cudaError_t e =
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       if (e != cudaSuccess) return e;
-      g_cache.attr_set[di][NR][kTma] = true;
+      g_cache.attr_set[di][NR][kTma][kBatch] = true;
     }
   }
   const int threads = 1 << (p.T - NR);
   if (threads > sweep_max_threads<R, NR>()) return cudaErrorInvalidConfiguration;
   // bulk copies move whole 16-byte multiples from 16-byte aligned addresses
   if (kTma && ((sizeof(A) << p.L) & 15u) != 0) return cudaErrorInvalidConfiguration;
-  const size_t smem = sweep_smem_bytes<R>(p.T, p.h, kTma, p.n_stages);
+  const size_t smem = sweep_smem_bytes<R>(p.T, p.h, kTma, p.n_stages) + (kBatch ? 128 : 0);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
   if (e != cudaSuccess) return e;
   per_sm = std::max(per_sm, 1);
-  const int64_t grid = std::min<int64_t>(p.tiles, (int64_t)sm_count * per_sm);
+  const int64_t grid = std::min<int64_t>(p.tiles * p.batch, (int64_t)sm_count * per_sm);
   kern<<<(unsigned)grid, threads, smem, s>>>(static_cast<A*>(state), p, err);
   return cudaGetLastError();
 }
@@ -601,10 +656,11 @@ template <typename R, int NR>
 cudaError_t launch_pick(void* state, const SweepParams<R>& p, int* err, int sm_count,
                         cudaStream_t s) {
   const uint32_t seg_bytes = (uint32_t)sizeof(typename Amp<R>::type) << p.L;
+  if (p.batch > 1 || p.n_local_slots > 0) return launch_nr<R, NR, false, true>(state, p, err, sm_count, s);
   // the bulk-copy store writes segments back where they came from: no relayout
   if (seg_bytes >= kTmaMinSegmentBytes && !p.relayout)
-    return launch_nr<R, NR, true>(state, p, err, sm_count, s);
-  return launch_nr<R, NR, false>(state, p, err, sm_count, s);
+    return launch_nr<R, NR, true, false>(state, p, err, sm_count, s);
+  return launch_nr<R, NR, false, false>(state, p, err, sm_count, s);
 }
 
 template <typename R>
@@ -652,6 +708,13 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
   p->n_stages = ns;
   p->relayout = sw.relayout;
   p->tiles = sw.tiles;
+  p->nq = sw.T + (int32_t)__builtin_ctzll((uint64_t)sw.tiles);
+  p->n_slots = 0;
+  p->tiles_log2 = (int32_t)__builtin_ctzll((uint64_t)sw.tiles);
+  p->pad2 = 0;
+  p->batch = 1;
+  p->paulis = nullptr;
+  p->n_local_slots = 0;
   for (int q = 0; q < SW_MAX_HIGH; ++q) {
     p->hq[q] = sw.hq[q];
     p->hs[q] = sw.hs[q];
@@ -689,6 +752,11 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
   for (int g = g_lo; g < g_hi; ++g) {
     SwGate sg = plan.gates[g];
     sg.moff -= pool_lo;
+    if (sg.kind == SK_PAULI) {  // slot -> local index into the staged choices
+      if (p->n_local_slots >= kSweepMaxGates) return false;
+      p->slot_map[p->n_local_slots] = sg.b;
+      sg.b = p->n_local_slots++;
+    }
     p->gates[g - g_lo] = sg;
   }
   // the pool slice of this sweep ends where the next sweep's first gate begins
@@ -714,6 +782,29 @@ cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int
   SweepParams<double> p;
   if (!fill_params(plan, k, &p)) return cudaErrorInvalidValue;
   return launch_t<double>(state, p, err, sm_count, s);
+}
+
+cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, const Plan& plan,
+                               size_t k, const uint8_t* paulis, int n_slots, int* err,
+                               int sm_count, cudaStream_t s) {
+  if (batch < 1 || ((uint64_t)plan.sweeps[k].tiles * (uint64_t)batch) > 0xffffffffull)
+    return cudaErrorInvalidValue;
+  auto fill = [&](auto* p) {
+    if (!fill_params(plan, k, p)) return false;
+    if (p->nq != n) return false;
+    p->batch = batch;
+    p->paulis = paulis;
+    p->n_slots = n_slots;
+    return true;
+  };
+  if (dtype == SC_C64) {
+    SweepParams<float> p;
+    if (!fill(&p)) return cudaErrorInvalidValue;
+    return launch_t<float>(states, p, err, sm_count, s);
+  }
+  SweepParams<double> p;
+  if (!fill(&p)) return cudaErrorInvalidValue;
+  return launch_t<double>(states, p, err, sm_count, s);
 }
 
 }  // namespace sc

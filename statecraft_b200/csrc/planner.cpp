@@ -22,6 +22,7 @@ double gate_cost(const PGate& g) {
     case PK_DENSE2: return 16.0;  // 4 complex MACs per amplitude
     case PK_DIAG1:
     case PK_DIAG2: return 3.0;    // 1 complex multiply + bit tests
+    case PK_PAULI: return 1.0;    // a register select / sign per trajectory
     default: return 0.5;          // register selects
   }
 }
@@ -39,6 +40,7 @@ int gate_pool_size(const PGate& g) {
 uint64_t dense_mask(const PGate& g) {
   switch (g.kind) {
     case PK_DENSE1:
+    case PK_PAULI:
     case PK_X: return 1ULL << g.q0;
     case PK_DENSE2:
     case PK_SWAP: return (1ULL << g.q0) | (1ULL << g.q1);
@@ -47,6 +49,7 @@ uint64_t dense_mask(const PGate& g) {
 }
 
 uint64_t touch_mask(const PGate& g) {
+  if (g.kind == PK_PAULI) return 1ULL << g.q0;
   uint64_t m = g.cmask | (1ULL << g.q0);
   if (g.kind == PK_DENSE2 || g.kind == PK_SWAP || g.kind == PK_DIAG2) m |= 1ULL << g.q1;
   return m;
@@ -467,7 +470,6 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     while (remaining > 0 || stage_list.empty()) {
       const bool first_stage = stage_list.empty();
       uint32_t R = 0;
-      uint32_t frozen = 0;  // positions moved by a folded permutation of this stage
       std::vector<int32_t> sg;
       for (size_t i = 0; i < list.size(); ++i) {
         if (staged[i]) continue;
@@ -483,8 +485,6 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
           const int q = __builtin_ctzll(m);
           if (pos_of[q] >= 0) touch |= 1u << pos_of[q];
         }
-        // data on frozen positions has logically moved already: wait for the next stage
-        if (touch & frozen) continue;
         uint32_t need = 0;
         for (uint64_t m = dense_mask(gates[g]); m; m &= m - 1)
           need |= 1u << pos_of[__builtin_ctzll(m)];
@@ -514,24 +514,35 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         if (first_stage && high_edges) want &= high_pos;
         if (popc(R) + popc(need) + popc(want) <= NR) need |= want;
         R |= need;
-        // X / CNOT / SWAP acting only on register bits is a register permutation:
-        // fold it into the stage's exit permutation instead of moving data
-        bool fold = false;
-        if (pw.kind == PK_SWAP) {
-          fold = true;
-        } else if (pw.kind == PK_X && (pw.cmask & ~tile_qmask) == 0 && popc(pw.cmask) <= 1) {
-          fold = pw.cmask == 0 || ((touch & ~R) == 0);
-        }
-        if (fold) {
-          folded[i] = 1;
-          frozen |= touch;
-        }
         sg.push_back((int32_t)i);
         staged[i] = 1;
       }
       if (sg.empty() && !first_stage) {  // cannot happen for a valid DAG
         plan.ok = false;
         return plan;
+      }
+      // X / CNOT / SWAP acting only on register bits is a register permutation: it
+      // is folded into the stage's exit permutation (no data moves) when no later
+      // gate of the stage touches its bits, and executed in registers otherwise
+      {
+        uint32_t later = 0;
+        for (size_t k = sg.size(); k-- > 0;) {
+          const int32_t i = sg[k];
+          const PGate& pw = gates[list[i]];
+          uint32_t touch = 0;
+          for (uint64_t m = touch_mask(pw); m; m &= m - 1) {
+            const int q = __builtin_ctzll(m);
+            if (pos_of[q] >= 0) touch |= 1u << pos_of[q];
+          }
+          bool fold = false;
+          if (pw.kind == PK_SWAP) {
+            fold = true;
+          } else if (pw.kind == PK_X && (pw.cmask & ~tile_qmask) == 0 && popc(pw.cmask) <= 1) {
+            fold = pw.cmask == 0 || ((touch & ~R) == 0);
+          }
+          if (fold && !(touch & later)) folded[i] = 1;
+          later |= touch;
+        }
       }
       remaining -= sg.size();
       stage_list.emplace_back(R, std::move(sg));
@@ -687,6 +698,11 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             sg.kind = SK_SWAP;
             sg.a = reg_of_pos[pos_of[pg.q0]];
             sg.b = reg_of_pos[pos_of[pg.q1]];
+            break;
+          case PK_PAULI:
+            sg.kind = SK_PAULI;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            sg.b = pg.q1;  // slot
             break;
           case PK_DIAG1:
             sg.kind = SK_D1;

@@ -230,6 +230,14 @@ uint64_t fresh_seed() {
 // ---------------------------------------------------------------------------
 namespace sc {
 
+int check_context(void* p) { return check_ctx(as_ctx(p)); }
+int validate_circuit(int n, const sc_op* ops, int64_t n_ops, int max_qubits) {
+  return validate_ops(n, ops, n_ops, max_qubits);
+}
+int validate_noise(const std::vector<sc_channel>& ch, const sc_op* ops, int64_t n_ops, int n) {
+  return validate_channels(ch, ops, n_ops, n);
+}
+
 PlanParams Ctx::plan_params() const {
   PlanParams pp;
   const bool c64 = cfg.dtype == SC_C64;

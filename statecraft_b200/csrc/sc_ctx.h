@@ -16,6 +16,11 @@ int fail(int code, const char* fmt, ...);
 int fail_cuda(cudaError_t e, const char* where);
 // frees a QAOA batch (sc_qaoa.cpp) and its device buffers
 void qaoa_batch_free(void* batch);
+// context handle check (also makes its device current) and the op / noise-record
+// validation of sc_run, shared with the batched entry points
+int check_context(void* ctx);
+int validate_circuit(int n, const sc_op* ops, int64_t n_ops, int max_qubits);
+int validate_noise(const std::vector<sc_channel>& ch, const sc_op* ops, int64_t n_ops, int n);
 
 struct DevBuf {
   void* p = nullptr;
@@ -53,6 +58,7 @@ struct Ctx {
   DevBuf buf_probs, buf_marg;                   // marginal probabilities
   DevBuf buf_expect;                            // Pauli partial sums
   DevBuf buf_adj_phi, buf_adj_lambda;           // adjoint work states
+  DevBuf buf_traj_states, buf_traj_aux;         // trajectory batches: states | codes, sampling
 
   // adjoint bookkeeping
   std::vector<sc_op> adj_ops;
@@ -85,7 +91,7 @@ struct Ctx {
   void release_all() {
     for (DevBuf* b : {&state, &buf_err, &buf_convert, &buf_noise_state,
                       &buf_noise_partial, &buf_sample, &buf_probs, &buf_marg, &buf_expect,
-                      &buf_adj_phi, &buf_adj_lambda})
+                      &buf_adj_phi, &buf_adj_lambda, &buf_traj_states, &buf_traj_aux})
       release(*b);
   }
   void mark_begin(int cls, double bytes, int kernels = 1);

@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "sc_rng.h"
+
 namespace sc {
 
 // Amplitude storage: complex128 = double2 (16 B), complex64 = float2 (8 B).
@@ -171,19 +173,6 @@ __device__ __forceinline__ void cp_async_wait() {
 
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// SplitMix64 (java.util.SplittableRandom): the k-th nextDouble() (k = 0, 1, ...)
-// of a generator seeded with `seed` is a pure function of (seed, k).
-__host__ __device__ __forceinline__ uint64_t splitmix_mix64(uint64_t z) {
-  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
-  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
-  return z ^ (z >> 31);
-}
-constexpr uint64_t kGoldenGamma = 0x9e3779b97f4a7c15ULL;
-__host__ __device__ __forceinline__ double splitmix_double(uint64_t seed, uint64_t k) {
-  const uint64_t z = splitmix_mix64(seed + (k + 1ULL) * kGoldenGamma);
-  return (double)(z >> 11) * 0x1.0p-53;
 }
 
 }  // namespace sc

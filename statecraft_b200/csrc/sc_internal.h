@@ -21,7 +21,9 @@ namespace sc {
 //   PK_SWAP    swap of qubits q0, q1                            -
 //   PK_DIAG1   diag(d0, d1) on q0, optionally controlled        m[0..3]
 //   PK_DIAG2   diag(d[4]) on (q0 = first, q1 = second)          m[0..7]
-enum PKind : int32_t { PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2 };
+//   PK_PAULI   Pauli slot on q0 (batched trajectories): the Pauli (I, X, Y or Z)
+//              is chosen per trajectory; q1 = slot index into the choice table
+enum PKind : int32_t { PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2, PK_PAULI };
 
 struct PGate {
   int32_t kind;
@@ -60,16 +62,18 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 // SK_D1R: uncontrolled diag(d0, d1) on register bit a.
 // SK_X0 / SK_CX0: SK_X / SK_CX without controls on tile positions outside the
 //        registers (a fixed register permutation).
+// SK_PAULI: Pauli slot on register bit a; b = slot, the Pauli of each trajectory
+//        comes from the sweep's choice table (0 = I, 1 = X, 2 = Y, 3 = Z).
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0
+  SK_X0, SK_CX0, SK_PAULI
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
 // register bits (< 4), kind << 4 otherwise.  The kernel switches on it once.
 inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
   switch (kind) {
-    case SK_G1: case SK_X: case SK_D1R: case SK_X0: return (kind << 4) | (a << 2);
+    case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: return (kind << 4) | (a << 2);
     case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0:
       return (kind << 4) | (a << 2) | b;
     default: return kind << 4;
@@ -186,11 +190,18 @@ cudaError_t launch_gate(int dtype, void* state, int n, const PGate& g, cudaStrea
 // bulk-copy wait times out
 cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int* err,
                          int sm_count, cudaStream_t s);
+// the same sweep over `batch` states of n qubits stored back to back; Pauli slots
+// read trajectory b's choice of slot j at paulis[b * n_slots + j]
+cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, const Plan& plan,
+                               size_t k, const uint8_t* paulis, int n_slots, int* err,
+                               int sm_count, cudaStream_t s);
 // in-place qubit-bit permutation of an n-qubit state
 cudaError_t launch_permute(int dtype, void* state, int n, const SwPerm& perm, int sm_count,
                            cudaStream_t s);
 // |0..0> or |basis>
 cudaError_t launch_init_basis(int dtype, void* state, int n, uint64_t basis, cudaStream_t s);
+// |0..0> in each of `batch` n-qubit states stored back to back
+cudaError_t launch_init_batch(int dtype, void* states, int n, int64_t batch, cudaStream_t s);
 // c128 host layout -> device amplitudes (dtype conversion for c64)
 cudaError_t launch_convert_in(int dtype, void* state, const double* src, int64_t count,
                               cudaStream_t s);

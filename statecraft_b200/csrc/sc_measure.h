@@ -38,4 +38,11 @@ cudaError_t launch_marginal(int dtype, const void* state, int n, uint64_t mmask,
 cudaError_t launch_sample(int dtype, const void* state, const double* probs, uint64_t len,
                           const SampleArgs& a, cudaStream_t s);
 
+// A batch of `batch` states of len amplitudes each, back to back: chunk sums /
+// prefixes / scalars per state (batch * sample_chunks(len), batch entries),
+// a.shots shots per state, state b drawing from SplittableRandom(a.seed + b);
+// outcomes[b * a.shots + k].
+cudaError_t launch_sample_batch(int dtype, const void* states, uint64_t len, int64_t batch,
+                                const SampleArgs& a, cudaStream_t s);
+
 }  // namespace sc

@@ -27,6 +27,14 @@ struct SweepParams {
   int32_t T, L, h, nr;
   int32_t n_stages, relayout;
   int64_t tiles;
+  // batched trajectories: `batch` states of 2^nq amplitudes back to back; Pauli
+  // slot j of state b applies paulis[b * n_slots + j]
+  int32_t nq, n_slots;
+  int32_t tiles_log2, pad2;
+  int64_t batch;
+  const uint8_t* paulis;
+  int32_t n_local_slots;                 // Pauli slots in this sweep
+  int32_t slot_map[kSweepMaxGates + 1];  // local slot -> slot index of the choice table
   int32_t hq[SW_MAX_HIGH];  // physical bit of tile position L + k (input layout)
   int32_t hs[SW_MAX_HIGH];  // the same bits ascending (tile enumeration)
   uint8_t outp[32];         // physical bit of tile position p in the output layout

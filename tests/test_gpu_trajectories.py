@@ -1,0 +1,122 @@
+"""Batched noisy trajectories on the GPU against the oracle's per-trajectory runs.
+
+The oracle runs each trajectory like StatevectorEngine.simulate: state-dependent
+Kraus branch weights, one nextDouble(total) per noise record from
+SplittableRandom(noise_seed + t), renormalisation.  Bars: identical branch choices;
+final states within 1e-12 (complex128) / 2e-5 (complex64) max-abs; outcome
+histograms identical when both sides sample the same uniforms, and within the
+total-variation bound max(0.01, 3 x TV between two disjoint-seed oracle batches).
+"""
+import numpy as np
+import pytest
+
+import randcirc as RCirc
+from oracle import oracle as O
+from statecraft_b200 import _abi as A
+from statecraft_b200 import noise as N
+from statecraft_b200 import workloads as W
+from statecraft_b200.engine import B200Config, NativeContext, serialize_channels, serialize_circuit
+from statecraft_b200.trajectories import (run_trajectories, total_variation,
+                                          touched_qubit_depolarizing)
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = NativeContext(B200Config())
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def ctx64():
+    c = NativeContext(B200Config(dtype=A.SC_C64))
+    yield c
+    c.close()
+
+
+def _oracle_trajectory(circuit, records, seed):
+    n = circuit.qubitCount
+    ops, n_ops = serialize_circuit(circuit)
+    ch, n_ch = serialize_channels(records)
+    st = O.initial_state(n)
+    rc, chosen = O.run(n, ops, n_ops, st, ch, n_ch, seed)
+    assert rc == 0
+    return st[0::2] + 1j * st[1::2], chosen
+
+
+@pytest.mark.parametrize("n,p", [(6, 0.3), (9, 0.1)])
+def test_ghz_choices_and_states_match_oracle(ctx, n, p):
+    c = W.ghz_circuit(n)
+    rec = touched_qubit_depolarizing(c, p)
+    res = run_trajectories(c, rec, 24, noise_seed=1000, shots=0, measure_seed=0,
+                           return_states=True, context=ctx)
+    for t in range(24):
+        want, chosen = _oracle_trajectory(c, rec, 1000 + t)
+        np.testing.assert_array_equal(res.choices[t], chosen)
+        np.testing.assert_allclose(res.states[t], want, rtol=0, atol=1e-12)
+    assert np.count_nonzero(res.choices) > 0  # some trajectories took Pauli branches
+
+
+def test_random_circuits_with_pauli_noise(ctx):
+    # dense gates, controlled gates and swaps with noise slots inside fused plans
+    for seed in range(3):
+        n = 11
+        c = RCirc.random_circuit(n, 60, seed=300 + seed)
+        rec = touched_qubit_depolarizing(c, 0.05)
+        res = run_trajectories(c, rec, 6, noise_seed=77 * seed, shots=0, measure_seed=0,
+                               return_states=True, context=ctx)
+        for t in range(6):
+            want, chosen = _oracle_trajectory(c, rec, 77 * seed + t)
+            np.testing.assert_array_equal(res.choices[t], chosen)
+            np.testing.assert_allclose(res.states[t], want, rtol=0, atol=1e-12)
+
+
+def test_complex64_trajectories(ctx64):
+    c = W.ghz_circuit(10)
+    rec = touched_qubit_depolarizing(c, 0.2)
+    res = run_trajectories(c, rec, 8, noise_seed=5, shots=0, measure_seed=0,
+                           return_states=True, context=ctx64)
+    for t in range(8):
+        want, chosen = _oracle_trajectory(c, rec, 5 + t)
+        np.testing.assert_array_equal(res.choices[t], chosen)
+        np.testing.assert_allclose(res.states[t], want, rtol=0, atol=2e-5)
+
+
+def test_histograms_match_oracle(ctx):
+    n, traj, shots = 12, 96, 64
+    c = W.ghz_circuit(n)
+    rec = touched_qubit_depolarizing(c, 0.02)
+    res = run_trajectories(c, rec, traj, noise_seed=4242, shots=shots, measure_seed=99,
+                           context=ctx)
+    oracle_out = []
+    for t in range(traj):
+        amp, _ = _oracle_trajectory(c, rec, 4242 + t)
+        st = np.empty(2 << n)
+        st[0::2], st[1::2] = amp.real, amp.imag
+        oracle_out.append(O.sample(st, n, list(range(n)), shots, 99 + t))
+    oracle_out = np.array(oracle_out)
+    # same uniforms on both sides: the outcomes agree except draws within 1e-12 of a
+    # CDF boundary (the two prefix sums round differently)
+    assert np.count_nonzero(res.outcomes != oracle_out) <= 2
+    # the total-variation bound against an oracle batch with disjoint seeds
+    other = []
+    for t in range(traj):
+        amp, _ = _oracle_trajectory(c, rec, 90000 + t)
+        st = np.empty(2 << n)
+        st[0::2], st[1::2] = amp.real, amp.imag
+        other.append(O.sample(st, n, list(range(n)), shots, 7000 + t))
+    h_gpu = res.histogram()
+    h_or = dict(zip(*np.unique(oracle_out, return_counts=True)))
+    h_other = dict(zip(*np.unique(np.array(other), return_counts=True)))
+    assert total_variation(h_gpu, h_or) <= max(0.01, 3 * total_variation(h_or, h_other))
+
+
+def test_non_pauli_channel_rejected(ctx):
+    c = W.ghz_circuit(4)
+    ad = N.AmplitudeDampingChannel(0.1, (0,))
+    kraus = tuple(np.array(k.matrix, dtype=complex).reshape(2, 2) for k in ad.krausDecomposition())
+    rec = [N.FlatChannel(0, 0, kraus)]
+    with pytest.raises(A.UnsupportedOperationException):
+        run_trajectories(c, rec, 4, noise_seed=1, shots=8, measure_seed=1, context=ctx)
