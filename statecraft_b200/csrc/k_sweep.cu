@@ -286,6 +286,9 @@ __device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
 #ifndef SC_SWEEP_C128_NR3_REGS
 #define SC_SWEEP_C128_NR3_REGS 96
 #endif
+#ifndef SC_SWEEP_C128_NR4_REGS
+#define SC_SWEEP_C128_NR4_REGS 168
+#endif
 
 template <typename R, int NR>
 constexpr int sweep_max_threads() {
@@ -294,8 +297,9 @@ constexpr int sweep_max_threads() {
 
 template <typename R, int NR>
 constexpr int sweep_max_regs() {
-  return NR == 3 && sizeof(R) == 8 ? SC_SWEEP_C128_NR3_REGS
-                                    : std::min(255, 65536 / sweep_max_threads<R, NR>());
+  return NR == 3 && sizeof(R) == 8   ? SC_SWEEP_C128_NR3_REGS
+         : NR == 4 && sizeof(R) == 8 ? SC_SWEEP_C128_NR4_REGS
+                                     : std::min(255, 65536 / sweep_max_threads<R, NR>());
 }
 
 constexpr long long kWaitLimitCycles = 2000000000LL;  // ~1 s at 2 GHz

@@ -241,11 +241,12 @@ int validate_noise(const std::vector<sc_channel>& ch, const sc_op* ops, int64_t 
 PlanParams Ctx::plan_params() const {
   PlanParams pp;
   const bool c64 = cfg.dtype == SC_C64;
-  pp.tile_qubits = cfg.tile_qubits > 0 ? cfg.tile_qubits : (c64 ? 11 : 10);
+  // 2048-amplitude tiles, 16 amplitudes per thread; no per-sweep FMA cap (the
+  // sweeps are issue-bound, so fewer, fuller sweeps save HBM passes for free)
+  pp.tile_qubits = cfg.tile_qubits > 0 ? cfg.tile_qubits : 11;
   pp.low_qubits = low_qubits > 0 ? low_qubits : (c64 ? 5 : 4);
-  pp.nr = nr > 0 ? nr : 3;
-  pp.budget = cfg.sweep_budget > 0 ? (double)cfg.sweep_budget
-                                   : (cfg.sweep_budget < 0 ? -1.0 : (c64 ? 160.0 : 96.0));
+  pp.nr = nr > 0 ? nr : 4;
+  pp.budget = cfg.sweep_budget > 0 ? (double)cfg.sweep_budget : -1.0;
   pp.max_gates = kSweepMaxGates;
   pp.max_pool = kSweepMaxPool;
   pp.relayout = relayout;
