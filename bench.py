@@ -50,6 +50,11 @@ def parse_args(argv=None):
     ap.add_argument("--sweep-budget", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--workload", choices=["statevector", "qaoa", "adjoint", "trajectories"],
+                    default="statevector",
+                    help="statevector: the headline line; the others time the batched "
+                         "QAOA, adjoint-gradient and noisy-trajectory workloads (one JSON "
+                         "line each, 1 GPU)")
     return ap.parse_args(argv)
 
 
@@ -175,6 +180,155 @@ def run_reference(args, rank: int) -> None:
 
 
 # ---------------------------------------------------------------------------
+# secondary workloads (one GPU; one JSON line each)
+# ---------------------------------------------------------------------------
+def _timed(fn, steps: int, warmup: int):
+    import torch
+
+    for _ in range(max(warmup, 0)):
+        fn()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        out = fn()
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / steps, out
+
+
+def run_qaoa(args) -> dict:
+    """4096 QAOA ring instances, n ~ U{10..22}, p = 4, one captured graph per evaluation."""
+    from statecraft_b200 import _abi as A
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.batch import QaoaRingBatch
+    from statecraft_b200.engine import B200Config, NativeContext
+
+    b = W.qaoa_instances(4096, 4, 4096)
+    ctx = NativeContext(B200Config())
+    res = {}
+    for name, dt in (("c128", A.SC_C128), ("c64", A.SC_C64)):
+        q = QaoaRingBatch(b.n_qubits, b.gammas, b.betas, dtype=dt, context=ctx)
+        sec, e = _timed(q.evaluate, args.steps, args.warmup)
+        info = q.info()
+        res[name] = {"s_per_batch": sec, "energies": e, "info": info,
+                     "hbm_gbs": info["hbm_bytes_per_run"] / sec / 1e9}
+        q.close()
+    ctx.close()
+    upd = QaoaRingBatch.amp_updates(b.n_qubits, 4)
+    err = np.abs(res["c64"]["energies"] - res["c128"]["energies"])
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    sec = res["c128"]["s_per_batch"]
+    return {"metric": "amp-updates/s (batched QAOA ring ansatz, 4096 instances, n ~ U{10..22}, p = 4, "
+                      "<sum ZZ> per instance, c128)",
+            "value": upd / sec, "unit": "amp-updates/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "qaoa-ring batch", "instances": 4096, "layers": 4,
+                       "n_range": [10, 22], "seed": 4096, "amp_updates_per_step": upd},
+            "instances_per_s": 4096 / sec,
+            "c128": {k: v for k, v in res["c128"].items() if k != "energies"},
+            "c64": {k: v for k, v in res["c64"].items() if k != "energies"},
+            "c64_energy_error_vs_c128": {"max": float(err.max()), "mean": float(err.mean())},
+            "roofline": {"bound": "hbm", "achieved": res["c128"]["hbm_gbs"], "peak": peak,
+                         "unit": "GB/s", "frac": res["c128"]["hbm_gbs"] / peak, "traffic": None}}
+
+
+def run_adjoint(args) -> dict:
+    """26-qubit hardware-efficient ansatz, 624 angles, 64-term Pauli sum: adjoint
+    gradients against central finite differences on the plain (forward) engine."""
+    from statecraft_b200 import _abi as A
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.adjoint import AdjointEngine
+    from statecraft_b200.engine import B200Config
+
+    n, layers, h = 26, 12, 1e-6
+    ops, n_ops, n_params = W.hea_ops(n, layers)
+    theta = W.hea_params(n_params, 2626)
+    x, z, c = W.random_pauli_sum(n, 64, 6464)
+    out = {}
+    for name, dt in (("c128", A.SC_C128), ("c64", A.SC_C64)):
+        eng = AdjointEngine(B200Config(dtype=dt))
+        sec, (e, g) = _timed(lambda: eng.value_and_grad(n, ops, n_ops, theta, x, z, c),
+                             args.steps, args.warmup)
+        out[name] = {"s_per_gradient": sec, "value": e, "grad": g}
+        eng.close()
+    # finite differences on the plain engine: the same circuit with the angles baked in
+    eng = AdjointEngine(B200Config())
+    idx = np.linspace(0, n_params - 1, 8).astype(int)
+    fd = []
+    t_eval = []
+    for k in idx:
+        vals = []
+        for sgn in (1, -1):
+            th = theta.copy()
+            th[k] += sgn * h
+            t0 = time.perf_counter()
+            vals.append(eng.expectation(n, ops, n_ops, th, x, z, c))
+            t_eval.append(time.perf_counter() - t0)
+        fd.append((vals[0] - vals[1]) / (2 * h))
+    eng.close()
+    fd = np.array(fd)
+    s_eval = float(np.median(t_eval))
+    fd_s = 2 * n_params * s_eval
+    g128 = out["c128"]["grad"]
+    diff = np.abs(g128[idx] - fd)
+    fd_noise = 4 * np.finfo(float).eps * float(np.sum(np.abs(c))) * n_ops / h
+    sec = out["c128"]["s_per_gradient"]
+    return {"metric": "adjoint gradients/s (26q c128 hardware-efficient ansatz, 12 layers, "
+                      "624 angles, 64-term Pauli sum) vs central finite differences",
+            "value": 1.0 / sec, "unit": "gradients/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "adjoint HEA", "qubits": n, "layers": layers,
+                       "angles": n_params, "terms": 64, "angle_seed": 2626, "h_seed": 6464},
+            "energy": out["c128"]["value"],
+            "finite_differences": {"h": h, "s_per_evaluation": s_eval,
+                                   "evaluations_per_gradient": 2 * n_params,
+                                   "gradients_per_s": 1.0 / fd_s,
+                                   "checked_angles": idx.tolist()},
+            "speedup_vs_fd": fd_s / sec,
+            "max_abs_diff_vs_fd": float(diff.max()), "fd_noise_bound": fd_noise,
+            "c64": {"gradients_per_s": 1.0 / out["c64"]["s_per_gradient"],
+                    "max_abs_grad_error_vs_c128": float(np.abs(out["c64"]["grad"] - g128).max()),
+                    "energy_error_vs_c128": abs(out["c64"]["value"] - out["c128"]["value"])}}
+
+
+def run_trajectories_bench(args) -> dict:
+    """Noisy 22-qubit GHZ, depolarizing p = 1e-3 after every gate on each touched
+    qubit, 1024 complex64 trajectories per batch, countsAll(64) each."""
+    from statecraft_b200 import _abi as A
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import B200Config, NativeContext
+    from statecraft_b200.trajectories import run_trajectories, touched_qubit_depolarizing
+
+    n, traj, shots = 22, 1024, 64
+    c = W.ghz_circuit(n)
+    rec = touched_qubit_depolarizing(c, 1e-3)
+    ctx = NativeContext(B200Config(dtype=A.SC_C64, timing=True))
+    sec, r = _timed(lambda: run_trajectories(c, rec, traj, 2024, shots, 4096, context=ctx),
+                    args.steps, args.warmup)
+    stats = {k: v for k, v in ctx.kernel_stats().items() if v["launches"]}
+    plan = ctx.plan_stats()
+    ctx.close()
+    sw = stats.get("sweep", {"ms": 0.0, "bytes": 0.0, "launches": 0})
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    gbs = sw["bytes"] / (sw["ms"] / 1e3) / 1e9 if sw["ms"] else None
+    h = r.histogram()
+    ghz = (h.get(0, 0) + h.get((1 << n) - 1, 0)) / (traj * shots)
+    return {"metric": "trajectories/s (noisy GHZ 22q c64, touched-qubit depolarizing p=1e-3, "
+                      "1024 trajectories x countsAll(64))",
+            "value": traj / sec, "unit": "trajectories/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "noisy GHZ trajectories", "qubits": n, "trajectories": traj,
+                       "shots": shots, "p": 1e-3, "noise_seed": 2024, "measure_seed": 4096,
+                       "noise_records": len(rec), "sweeps": plan["sweeps"]},
+            "kernel_stats": stats,
+            "ghz_fraction": ghz,
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": (gbs / peak) if gbs else None, "traffic": None}}
+
+
+# ---------------------------------------------------------------------------
 # the B200 engine
 # ---------------------------------------------------------------------------
 def main(argv=None) -> int:
@@ -184,6 +338,11 @@ def main(argv=None) -> int:
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank)
+        return 0
+    if args.workload != "statevector":
+        fn = {"qaoa": run_qaoa, "adjoint": run_adjoint,
+              "trajectories": run_trajectories_bench}[args.workload]
+        print(json.dumps(fn(args)), flush=True)
         return 0
 
     import torch

@@ -307,6 +307,48 @@ def test_adjoint_gradient_matches_parameter_shift(n, layers):
     eng.close()
 
 
+def test_adjoint_gradient_matches_central_differences():
+    # the FP64 check of the adjoint method against central finite differences (h = 1e-6)
+    # on the plain forward engine; FD round-off sets the tolerance
+    from statecraft_b200.adjoint import AdjointEngine
+
+    n, layers, h = 14, 3, 1e-6
+    ops, n_ops, n_params = W.hea_ops(n, layers)
+    params = W.hea_params(n_params, seed=2626)
+    x, z, c = W.random_pauli_sum(n, 24, seed=6464)
+    eng = AdjointEngine()
+    _, g = eng.value_and_grad(n, ops, n_ops, params, x, z, c)
+    fd = np.zeros(n_params)
+    for k in range(n_params):
+        vals = []
+        for s in (h, -h):
+            p = params.copy()
+            p[k] += s
+            vals.append(eng.expectation(n, ops, n_ops, p, x, z, c))
+        fd[k] = (vals[0] - vals[1]) / (2 * h)
+    noise = 4 * np.finfo(float).eps * float(np.sum(np.abs(c))) * n_ops / h
+    np.testing.assert_allclose(g, fd, rtol=0, atol=max(1e-8, noise))
+    eng.close()
+
+
+def test_adjoint_complex64_error_reported():
+    from statecraft_b200.adjoint import AdjointEngine
+
+    n, layers = 12, 3
+    ops, n_ops, n_params = W.hea_ops(n, layers)
+    params = W.hea_params(n_params, seed=2626)
+    x, z, c = W.random_pauli_sum(n, 16, seed=6464)
+    e128 = AdjointEngine()
+    e64 = AdjointEngine(B200Config(dtype=A.SC_C64))
+    v1, g1 = e128.value_and_grad(n, ops, n_ops, params, x, z, c)
+    v2, g2 = e64.value_and_grad(n, ops, n_ops, params, x, z, c)
+    err = float(np.max(np.abs(g1 - g2)))
+    print("complex64 adjoint: |dE| = %.3e, max |d grad| = %.3e" % (abs(v1 - v2), err))
+    assert abs(v1 - v2) < 1e-4 and err < 1e-4
+    e128.close()
+    e64.close()
+
+
 # ---- full-size properties ---------------------------------------------------------
 def test_28q_brickwall_fused_matches_unfused():
     c = W.brickwall_circuit(28, 4, seed=3030, mcz=True, rzz=True)
