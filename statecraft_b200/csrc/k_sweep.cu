@@ -45,8 +45,23 @@ __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R*
     const int j1 = j | (1 << A_);
     if (lmask && (((l0 | off[j]) & lmask) != lmask)) continue;
     const auto a0 = v[j], a1 = v[j1];
-    v[j] = cmac2(m00r, m00i, a0, m01r, m01i, a1);
-    v[j1] = cmac2(m10r, m10i, a0, m11r, m11i, a1);
+    // every use of a0 comes before any use of a1 and the last use of a1 completes
+    // each output, so the outputs can take the inputs' registers in place
+    R o0x = m00r * a0.x, o0y = m00r * a0.y, o1x = m10r * a0.x, o1y = m10r * a0.y;
+    o0x = fma(-m00i, a0.y, o0x);
+    o0y = fma(m00i, a0.x, o0y);
+    o1x = fma(-m10i, a0.y, o1x);
+    o1y = fma(m10i, a0.x, o1y);
+    o0x = fma(m01r, a1.x, o0x);
+    o0y = fma(m01r, a1.y, o0y);
+    o1x = fma(m11r, a1.x, o1x);
+    o1y = fma(m11r, a1.y, o1y);
+    o0x = fma(-m01i, a1.y, o0x);
+    o0y = fma(m01i, a1.x, o0y);
+    o1x = fma(-m11i, a1.y, o1x);
+    o1y = fma(m11i, a1.x, o1y);
+    v[j] = make_amp<R>(o0x, o0y);
+    v[j1] = make_amp<R>(o1x, o1y);
   }
 }
 
@@ -197,6 +212,27 @@ __device__ __forceinline__ void d1r(typename Amp<R>::type (&v)[1 << NR], const R
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j)
     v[j] = ((j >> A_) & 1) ? cmul(d1r_, d1i_, v[j]) : cmul(d0r, d0i, v[j]);
+}
+
+// uncontrolled 2x2 gates on the register bits of mask M (ascending; matrices
+// consecutive in the pool)
+template <typename R, int NR, int M>
+__device__ __forceinline__ void g1all(typename Amp<R>::type (&v)[1 << NR], const R* m,
+                                      uint32_t l0, const uint32_t (&off)[1 << NR]) {
+  const R* mm = m;
+  if constexpr ((M & 1) != 0) {
+    g1<R, NR, 0>(v, mm, l0, off, 0u);
+    mm += 8;
+  }
+  if constexpr (NR > 1 && (M & 2) != 0) {
+    g1<R, NR, 1>(v, mm, l0, off, 0u);
+    mm += 8;
+  }
+  if constexpr (NR > 2 && (M & 4) != 0) {
+    g1<R, NR, 2>(v, mm, l0, off, 0u);
+    mm += 8;
+  }
+  if constexpr (NR > 3 && (M & 8) != 0) g1<R, NR, 3>(v, mm, l0, off, 0u);
 }
 
 // Pauli chosen per trajectory on register bit A_: 1 = X, 2 = Y, 3 = Z (the
@@ -514,28 +550,19 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #undef SC_DO_CX
 #undef SC_DO_DPR
 #undef SC_DO_SWAP
-          case SK_G1ALL << 4: {
-            // commuting 2x2 gates on several register bits, matrices in bit order
-            const int mask = g.a;
-            const R* mm = m;
-            if (mask & 1) {
-              g1<R, NR, 0>(v, mm, l0, off, 0u);
-              mm += 8;
-            }
-            if constexpr (NR > 1)
-              if (mask & 2) {
-                g1<R, NR, 1>(v, mm, l0, off, 0u);
-                mm += 8;
-              }
-            if constexpr (NR > 2)
-              if (mask & 4) {
-                g1<R, NR, 2>(v, mm, l0, off, 0u);
-                mm += 8;
-              }
-            if constexpr (NR > 3)
-              if (mask & 8) g1<R, NR, 3>(v, mm, l0, off, 0u);
-            break;
-          }
+          // commuting 2x2 gates on several register bits, matrices in bit order;
+          // one case per bit set, so the gates run as straight-line code
+#define SC_G1ALL_CASE(M)                        \
+  case (SK_G1ALL << 4) | (M):                   \
+    if constexpr (((M) >> NR) == 0) {           \
+      g1all<R, NR, (M)>(v, m, l0, off);         \
+    }                                           \
+    break;
+          SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
+          SC_G1ALL_CASE(5) SC_G1ALL_CASE(6) SC_G1ALL_CASE(7) SC_G1ALL_CASE(8)
+          SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
+          SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
+#undef SC_G1ALL_CASE
           case SK_D1 << 4: {
             // diag(d0, d1) on one bit; the bit is a tile position (a >= 0) or a
             // global qubit fixed for the whole tile (a < 0)
@@ -771,6 +798,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
   }
   if (pool_hi - pool_lo > kSweepMaxPool) return false;
   for (int32_t e = pool_lo; e < pool_hi; ++e) p->pool[e - pool_lo] = (R)plan.pool[e];
+  p->pool_len = pool_hi - pool_lo;
   return true;
 }
 

@@ -70,12 +70,14 @@ enum SwKind : int32_t {
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
-// register bits (< 4), kind << 4 otherwise.  The kernel switches on it once.
+// register bits (< 4), kind << 4 | mask for SK_G1ALL, kind << 4 otherwise.  The
+// kernel switches on it once.
 inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
   switch (kind) {
     case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: return (kind << 4) | (a << 2);
     case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0:
       return (kind << 4) | (a << 2) | b;
+    case SK_G1ALL: return (kind << 4) | (a & 15);  // a = register-bit mask
     default: return kind << 4;
   }
 }

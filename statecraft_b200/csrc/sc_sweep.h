@@ -33,6 +33,7 @@ struct SweepParams {
   int32_t tiles_log2, pad2;
   int64_t batch;
   const uint8_t* paulis;
+  int32_t pool_len;                      // matrix reals of this sweep (staged in shared memory)
   int32_t n_local_slots;                 // Pauli slots in this sweep
   int32_t slot_map[kSweepMaxGates + 1];  // local slot -> slot index of the choice table
   int32_t hq[SW_MAX_HIGH];  // physical bit of tile position L + k (input layout)
