@@ -91,7 +91,7 @@ __global__ void __launch_bounds__(1 << (kQT - NR), MB)
   extern __shared__ __align__(16) unsigned char smem_raw[];
   A* const tiles = reinterpret_cast<A*>(smem_raw);
   A* const ph = tiles + (DB ? 2 : 1) * kTile;
-  R* const rxc = reinterpret_cast<R*>(ph + a.p * (kQaoaMaxQubits + 1));  // (cos, sin) per layer
+  R* const rxc = reinterpret_cast<R*>(ph + a.p * (kQaoaMaxQubits + 1));  // (t, form) per layer
   double* const red = reinterpret_cast<double*>(rxc + 2 * kQaoaMaxLayers);
   const uint32_t t = threadIdx.x;
   A* const st = static_cast<A*>(a.state);
@@ -221,24 +221,35 @@ __global__ void __launch_bounds__(1 << (kQT - NR), MB)
       for (int j = 0; j < NV; ++j) v[j] = cur[sbase[G] ^ qslot<R, NR>((uint32_t)j << (G * NR))];
       gcur = G;
     };
-    // RX(2 beta) = [[cos b, -i sin b], [-i sin b, cos b]] on the gate bits of the layout
+    // RX(2 beta) = [[c, -i s], [-i s, c]] up to a scalar: c (I - i t X) with
+    // t = s / c when |c| >= |s| (form 0), else s (u I - i X) with u = c / s
+    // (form 1); |t|, |u| <= 1.  One FMA per output component; the scalars of a
+    // whole layer half are folded into the phase tables / final energy on the host.
     auto rx = [&](int l) {
-      const R cb = rxc[2 * l], sb = rxc[2 * l + 1];
+      const R tq = rxc[2 * l];
+      const bool form1 = rxc[2 * l + 1] != (R)0;
       const uint32_t rm = (smask >> (gcur * NR)) & (uint32_t)(NV - 1);
 #pragma unroll
       for (int k = 0; k < NR; ++k) {
         if (!((rm >> k) & 1u)) continue;
+        if (!form1) {
 #pragma unroll
-        for (int j = 0; j < NV; ++j) {
-          if (j & (1 << k)) continue;
-          const A a0 = v[j], a1 = v[j | (1 << k)];
-          A n0, n1;
-          n0.x = cb * a0.x + sb * a1.y;
-          n0.y = cb * a0.y - sb * a1.x;
-          n1.x = sb * a0.y + cb * a1.x;
-          n1.y = cb * a1.y - sb * a0.x;
-          v[j] = n0;
-          v[j | (1 << k)] = n1;
+          for (int j = 0; j < NV; ++j) {
+            if (j & (1 << k)) continue;
+            const A a0 = v[j], a1 = v[j | (1 << k)];
+            // (I - i t X): n0 = a0 - i t a1, n1 = a1 - i t a0
+            v[j] = make_amp<R>(fma(tq, a1.y, a0.x), fma(-tq, a1.x, a0.y));
+            v[j | (1 << k)] = make_amp<R>(fma(tq, a0.y, a1.x), fma(-tq, a0.x, a1.y));
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < NV; ++j) {
+            if (j & (1 << k)) continue;
+            const A a0 = v[j], a1 = v[j | (1 << k)];
+            // (u I - i X): n0 = u a0 - i a1, n1 = u a1 - i a0
+            v[j] = make_amp<R>(fma(tq, a0.x, a1.y), fma(tq, a0.y, -a1.x));
+            v[j | (1 << k)] = make_amp<R>(fma(tq, a1.x, a0.y), fma(tq, a1.y, -a0.x));
+          }
         }
       }
     };
@@ -336,6 +347,9 @@ __global__ void __launch_bounds__(1 << (kQT - NR), MB)
           n_acc += p2;
         }
       });
+      const double es = a.escale[in.orig];  // squared scalar of the last RX half
+      e_acc *= es;
+      n_acc *= es;
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         e_acc += __shfl_xor_sync(0xffffffffu, e_acc, o);

@@ -31,8 +31,8 @@ struct QaoaBatch {
   int64_t n_items_large = 0;
   int64_t arena_amps = 0;
   int64_t n_phase = 0;  // complex entries
-  DevBuf d_state, d_large, d_whole, d_lprefix, d_wprefix, d_cs, d_phase, d_partials, d_spans,
-      d_energy, d_norm;
+  DevBuf d_state, d_large, d_whole, d_lprefix, d_wprefix, d_cs, d_escale, d_phase, d_partials,
+      d_spans, d_energy, d_norm;
   int shape = 1;
   int ctas = 1;
   double tuned_ms = 0.0;
@@ -45,8 +45,8 @@ struct QaoaBatch {
     if (graph) cudaGraphDestroy(graph);
     exec = nullptr;
     graph = nullptr;
-    for (DevBuf* b : {&d_state, &d_large, &d_whole, &d_lprefix, &d_wprefix, &d_cs, &d_phase,
-                      &d_partials, &d_spans, &d_energy, &d_norm})
+    for (DevBuf* b : {&d_state, &d_large, &d_whole, &d_lprefix, &d_wprefix, &d_cs, &d_escale,
+                      &d_phase, &d_partials, &d_spans, &d_energy, &d_norm})
       ctx->release(*b);
   }
 };
@@ -76,31 +76,70 @@ int upload(Ctx* c, DevBuf& b, const void* src, size_t bytes, const char* what) {
   return e == cudaSuccess ? SC_OK : fail_cuda(e, what);
 }
 
-// RX coefficients and cost-phase tables from the angles, in FP64 on the host
+// RX coefficients and cost-phase tables from the angles, in FP64 on the host.
+//
+// RX(2b) = c I - i s X (c = cos b, s = sin b) is applied as a scalar times a
+// matrix with one unit diagonal or off-diagonal: c (I - i t X), t = s / c, when
+// |c| >= |s|, else s (u I - i X), u = c / s.  A layer half acting on k qubits then
+// leaves the scalar sc^k, which is folded into the next cost-phase table (a
+// pass applies RX of layer l-1 on its half, the phase of layer l, RX of layer l
+// on its half) or, after the last layer, into the energy (squared).
 int fill_angles(QaoaBatch* q, const double* gammas, const double* betas) {
-  std::vector<double> cs(2 * (size_t)q->n_inst * q->p);
+  const int p = q->p;
+  std::vector<double> cs(2 * (size_t)q->n_inst * p);
+  std::vector<double> scal((size_t)q->n_inst * p);
   std::vector<double> ph(2 * (size_t)q->n_phase);
-  auto put_tables = [&](const QaoaInst& in) {
-    for (int l = 0; l < q->p; ++l) {
-      const double g = gammas[(size_t)in.orig * q->p + l];
+  std::vector<double> escale((size_t)q->n_inst, 1.0);
+  for (int64_t i = 0; i < q->n_inst; ++i)
+    for (int l = 0; l < p; ++l) {
+      const double b = betas[(size_t)i * p + l];
+      const double c = std::cos(b), s = std::sin(b);
+      const size_t at = (size_t)i * p + l;
+      if (std::fabs(c) >= std::fabs(s)) {
+        cs[2 * at] = s / c;
+        cs[2 * at + 1] = 0.0;
+        scal[at] = c;
+      } else {
+        cs[2 * at] = c / s;
+        cs[2 * at + 1] = 1.0;
+        scal[at] = s;
+      }
+    }
+  // half_bits(k): qubits the RX layers of pass k act on; whole instances apply
+  // every layer to all n qubits in one go
+  auto put_tables = [&](const QaoaInst& in, bool whole) {
+    const size_t base = (size_t)in.orig * p;
+    auto half_bits = [&](int k) {
+      if (whole) return in.n;
+      return (k & 1) ? in.n - kQaoaTileQubits : kQaoaTileQubits;
+    };
+    for (int l = 0; l < p; ++l) {
+      const double g = gammas[base + l];
+      // scalars folded into this table: RX of layer l-1 and (pass form) layer l
+      double f = 1.0;
+      if (whole) {
+        if (l > 0) f = std::pow(scal[base + l - 1], in.n);
+      } else {
+        const int bits = half_bits(l);
+        f = std::pow(scal[base + l], bits);
+        if (l > 0) f *= std::pow(scal[base + l - 1], bits);
+      }
       for (int k = 0; k <= in.n; ++k) {
         // exp(-i gamma sum_j z_j z_{j+1}) with sum = n - 2k
         const double a = -g * (double)(in.n - 2 * k);
         const size_t at = 2 * (size_t)(in.ph_off + (int64_t)l * (in.n + 1) + k);
-        ph[at] = std::cos(a);
-        ph[at + 1] = std::sin(a);
+        ph[at] = f * std::cos(a);
+        ph[at + 1] = f * std::sin(a);
       }
     }
+    const double last = std::pow(scal[base + p - 1], whole ? in.n : half_bits(p));
+    escale[in.orig] = last * last;
   };
-  for (const QaoaInst& in : q->large) put_tables(in);
-  for (const QaoaInst& in : q->whole) put_tables(in);
-  for (int64_t i = 0; i < q->n_inst; ++i)
-    for (int l = 0; l < q->p; ++l) {
-      const double b = betas[(size_t)i * q->p + l];  // RX(2b): cos b, sin b
-      cs[2 * ((size_t)i * q->p + l)] = std::cos(b);
-      cs[2 * ((size_t)i * q->p + l) + 1] = std::sin(b);
-    }
+  for (const QaoaInst& in : q->large) put_tables(in, false);
+  for (const QaoaInst& in : q->whole) put_tables(in, true);
   int rc = upload(q->ctx, q->d_cs, cs.data(), cs.size() * sizeof(double), "QAOA RX table");
+  if (rc == SC_OK)
+    rc = upload(q->ctx, q->d_escale, escale.data(), escale.size() * sizeof(double), "QAOA scales");
   if (rc != SC_OK) return rc;
   return upload(q->ctx, q->d_phase, ph.data(), ph.size() * sizeof(double), "QAOA phase table");
 }
@@ -113,6 +152,7 @@ int enqueue(QaoaBatch* q, int shape, int ctas) {
   a.state = q->d_state.p;
   a.p = q->p;
   a.cs = static_cast<const double*>(q->d_cs.p);
+  a.escale = static_cast<const double*>(q->d_escale.p);
   a.phase = static_cast<const double*>(q->d_phase.p);
   a.partials = static_cast<double*>(q->d_partials.p);
   if (!q->whole.empty()) {

@@ -50,7 +50,8 @@ struct QaoaLaunch {
   int32_t n_inst;
   int32_t p;
   int64_t n_items;
-  const double* cs;            // (cos beta, sin beta) at 2 * (orig * p + l)
+  const double* cs;            // RX (t, form) at 2 * (orig * p + l), see sc_qaoa.cpp
+  const double* escale;        // per instance: energy / norm factor of the last RX scalars
   const double* phase;         // (re, im) pairs
   double* partials;            // (energy, norm) per item
   int64_t part_base;           // partial slot of item 0
