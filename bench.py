@@ -55,6 +55,9 @@ def parse_args(argv=None):
                     help="statevector: the headline line; the others time the batched "
                          "QAOA, adjoint-gradient and noisy-trajectory workloads (one JSON "
                          "line each, 1 GPU)")
+    ap.add_argument("--instances", type=int, default=4096, help="QAOA batch size")
+    ap.add_argument("--trajectories", type=int, default=1024, help="trajectory batch size")
+    ap.add_argument("--no-tune", action="store_true", help="QAOA: fixed kernel shape")
     return ap.parse_args(argv)
 
 
@@ -202,11 +205,13 @@ def run_qaoa(args) -> dict:
     from statecraft_b200.batch import QaoaRingBatch
     from statecraft_b200.engine import B200Config, NativeContext
 
-    b = W.qaoa_instances(4096, 4, 4096)
+    count = args.instances
+    b = W.qaoa_instances(count, 4, 4096)
     ctx = NativeContext(B200Config())
     res = {}
     for name, dt in (("c128", A.SC_C128), ("c64", A.SC_C64)):
-        q = QaoaRingBatch(b.n_qubits, b.gammas, b.betas, dtype=dt, context=ctx)
+        q = QaoaRingBatch(b.n_qubits, b.gammas, b.betas, dtype=dt, tune=not args.no_tune,
+                          context=ctx)
         sec, e = _timed(q.evaluate, args.steps, args.warmup)
         info = q.info()
         res[name] = {"s_per_batch": sec, "energies": e, "info": info,
@@ -217,14 +222,14 @@ def run_qaoa(args) -> dict:
     err = np.abs(res["c64"]["energies"] - res["c128"]["energies"])
     peak = measured_peaks().get("hbm_gbs") or 6650.0
     sec = res["c128"]["s_per_batch"]
-    return {"metric": "amp-updates/s (batched QAOA ring ansatz, 4096 instances, n ~ U{10..22}, p = 4, "
-                      "<sum ZZ> per instance, c128)",
+    return {"metric": f"amp-updates/s (batched QAOA ring ansatz, {count} instances, n ~ U{{10..22}}, "
+                      "p = 4, <sum ZZ> per instance, c128)",
             "value": upd / sec, "unit": "amp-updates/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "qaoa-ring batch", "instances": 4096, "layers": 4,
+            "config": {"workload": "qaoa-ring batch", "instances": count, "layers": 4,
                        "n_range": [10, 22], "seed": 4096, "amp_updates_per_step": upd},
-            "instances_per_s": 4096 / sec,
+            "instances_per_s": count / sec,
             "c128": {k: v for k, v in res["c128"].items() if k != "energies"},
             "c64": {k: v for k, v in res["c64"].items() if k != "energies"},
             "c64_energy_error_vs_c128": {"max": float(err.max()), "mean": float(err.mean())},
@@ -300,7 +305,7 @@ def run_trajectories_bench(args) -> dict:
     from statecraft_b200.engine import B200Config, NativeContext
     from statecraft_b200.trajectories import run_trajectories, touched_qubit_depolarizing
 
-    n, traj, shots = 22, 1024, 64
+    n, traj, shots = 22, args.trajectories, 64
     c = W.ghz_circuit(n)
     rec = touched_qubit_depolarizing(c, 1e-3)
     ctx = NativeContext(B200Config(dtype=A.SC_C64, timing=True))
@@ -314,8 +319,8 @@ def run_trajectories_bench(args) -> dict:
     gbs = sw["bytes"] / (sw["ms"] / 1e3) / 1e9 if sw["ms"] else None
     h = r.histogram()
     ghz = (h.get(0, 0) + h.get((1 << n) - 1, 0)) / (traj * shots)
-    return {"metric": "trajectories/s (noisy GHZ 22q c64, touched-qubit depolarizing p=1e-3, "
-                      "1024 trajectories x countsAll(64))",
+    return {"metric": f"trajectories/s (noisy GHZ 22q c64, touched-qubit depolarizing p=1e-3, "
+                      f"{traj} trajectories x countsAll(64))",
             "value": traj / sec, "unit": "trajectories/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
