@@ -215,6 +215,35 @@ bool is_parity_diag(const PGate& g) {
   return g.m[0] == g.m[6] && g.m[1] == g.m[7] && g.m[2] == g.m[4] && g.m[3] == g.m[5];
 }
 
+// A 2x2 unitary u as e^{ig} c diag(1, e^{i phi}) [[1, -t], [t, 1]] diag(1, e^{i lam})
+// with c = |u00| >= min_c, s = |u10| > 0, t = s / c (u00 = e^{ig} c,
+// u01 = -e^{ig} e^{i lam} s, u10 = e^{ig} e^{i phi} s, u11 = e^{ig} e^{i(phi+lam)} c).
+// q = {t, Re e^{i lam}, Im e^{i lam}, Re e^{i phi}, Im e^{i phi}}; (fr, fi) = e^{ig} c.
+// False when u is not of that form (not unitary to 1e-13, c too small, s = 0).
+bool rotation_form(const double* u, double min_c, double* q, double* fr, double* fi) {
+  const double c = std::hypot(u[0], u[1]), s = std::hypot(u[4], u[5]);
+  if (!(min_c > 0.0) || !(c >= min_c) || !(s > 0.0)) return false;
+  if (std::fabs(c * c + s * s - 1.0) > 1e-13 || std::fabs(std::hypot(u[2], u[3]) - s) > 1e-13 ||
+      std::fabs(std::hypot(u[6], u[7]) - c) > 1e-13)
+    return false;
+  const double gr = u[0] / c, gi = u[1] / c;  // e^{ig}
+  // e^{i phi} = u10 conj(e^{ig}) / s, e^{i lam} = -u01 conj(e^{ig}) / s
+  const double pr = (u[4] * gr + u[5] * gi) / s, pi = (u[5] * gr - u[4] * gi) / s;
+  const double lr = -(u[2] * gr + u[3] * gi) / s, li = -(u[3] * gr - u[2] * gi) / s;
+  // u11 must equal e^{ig} e^{i phi} e^{i lam} c
+  const double plr = pr * lr - pi * li, pli = pr * li + pi * lr;
+  const double er = c * (gr * plr - gi * pli), ei = c * (gr * pli + gi * plr);
+  if (std::fabs(er - u[6]) > 1e-13 || std::fabs(ei - u[7]) > 1e-13) return false;
+  q[0] = s / c;
+  q[1] = lr;
+  q[2] = li;
+  q[3] = pr;
+  q[4] = pi;
+  *fr = gr * c;
+  *fi = gi * c;
+  return true;
+}
+
 // In-place bit permutations that take the layout phys_of back to the identity:
 // transpositions of physical bits, grouped while their bits (plus the low bits,
 // which keep the copies coalesced) fit one permutation tile.
@@ -388,6 +417,8 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     SwSweep sw;
     std::memset(&sw, 0, sizeof sw);
     sw.T = T; sw.L = L; sw.h = h; sw.nr = NR;
+    sw.scale_re = 1.0;
+    sw.scale_im = 0.0;
     sw.tiles = 1LL << (n - T);
     int pos_of[64];
     int log_at[32];  // logical qubit at each tile position
@@ -601,6 +632,40 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         SwGate sg;
         std::memset(&sg, 0, sizeof sg);
         sg.moff = (int32_t)plan.pool.size();
+        // rotation form when every gate of the run has one
+        {
+          std::sort(run.begin(), run.end(),
+                    [](const std::pair<int, const double*>& x, const std::pair<int, const double*>& y) {
+                      return x.first < y.first;
+                    });
+          std::vector<double> qs;
+          double sr = sw.scale_re, si = sw.scale_im;
+          bool all = true;
+          for (const auto& r : run) {
+            double q[5], fr, fi;
+            if (!rotation_form(r.second, pp.rot_min_c, q, &fr, &fi)) {
+              all = false;
+              break;
+            }
+            qs.insert(qs.end(), q, q + 5);
+            const double nr = sr * fr - si * fi, ni = sr * fi + si * fr;
+            sr = nr;
+            si = ni;
+          }
+          if (all) {
+            sg.kind = SK_G1ALLQ;
+            for (const auto& r : run) sg.a |= 1 << r.first;
+            plan.pool.insert(plan.pool.end(), qs.begin(), qs.end());
+            sw.scale_re = sr;
+            sw.scale_im = si;
+            sg.code = sw_code(sg.kind, sg.a, sg.b);
+            plan.gates.push_back(sg);
+            plan.gate_ops.insert(plan.gate_ops.end(), run_ops.begin(), run_ops.end());
+            run.clear();
+            run_ops.clear();
+            return;
+          }
+        }
         if (run.size() == 1) {
           sg.kind = SK_G1;
           sg.a = run[0].first;

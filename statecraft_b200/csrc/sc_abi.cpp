@@ -250,6 +250,9 @@ PlanParams Ctx::plan_params() const {
   pp.max_gates = kSweepMaxGates;
   pp.max_pool = kSweepMaxPool;
   pp.relayout = relayout;
+  // rotation form for 1-qubit unitaries: |u00| >= 0.05 (c128) / 0.25 (c64) keeps
+  // t <= 20 / 4 and a sweep's scalar far from under- or overflow
+  pp.rot_min_c = rotation ? (c64 ? 0.25 : 0.05) : 0.0;
   return pp;
 }
 
@@ -463,6 +466,7 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
   if (const char* v = getenv("STATECRAFT_B200_LOW_QUBITS")) c->low_qubits = atoi(v);
   if (const char* v = getenv("STATECRAFT_B200_NR")) c->nr = atoi(v);
   if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) c->relayout = atoi(v) != 0;
+  if (const char* v = getenv("STATECRAFT_B200_ROTATION")) c->rotation = atoi(v) != 0;
   *out_ctx = c;
   return SC_OK;
 }

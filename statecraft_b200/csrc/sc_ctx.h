@@ -38,6 +38,7 @@ struct Ctx {
   int low_qubits = 0;  // planner overrides (0 = default)
   int nr = 0;
   bool relayout = true;
+  bool rotation = true;  // rotation form for 1-qubit unitaries in sweeps
 
   // state
   int n = 0;

@@ -27,6 +27,8 @@ PlanParams debug_params(int tile, int low, int nr, double budget) {
   pp.max_gates = kSweepMaxGates;
   pp.max_pool = kSweepMaxPool;
   if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) pp.relayout = atoi(v) != 0;
+  pp.rot_min_c = 0.05;
+  if (const char* v = getenv("STATECRAFT_B200_ROTATION")) pp.rot_min_c = atoi(v) != 0 ? 0.05 : 0.0;
   return pp;
 }
 
@@ -192,6 +194,24 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
               }
               break;
             }
+            case SK_G1ALLQ: {
+              const double* q = m;
+              for (int bit = 0; bit < NR; ++bit) {
+                if (!((g.a >> bit) & 1)) continue;
+                const double t = q[0], lr = q[1], li = q[2], pr = q[3], pi = q[4];
+                for (int j = 0; j < NV; ++j) {
+                  if (j & (1 << bit)) continue;
+                  const int j1 = j | (1 << bit);
+                  const C a0 = v[j], a1 = v[j1];
+                  const C b1 = {lr * a1.r - li * a1.i, lr * a1.i + li * a1.r};
+                  const C m1 = {t * a0.r + b1.r, t * a0.i + b1.i};
+                  v[j] = {a0.r - t * b1.r, a0.i - t * b1.i};
+                  v[j1] = {pr * m1.r - pi * m1.i, pr * m1.i + pi * m1.r};
+                }
+                q += 5;
+              }
+              break;
+            }
             case SK_D1R:
               for (int j = 0; j < NV; ++j) {
                 const int k = (j >> g.a) & 1;
@@ -225,8 +245,9 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
       }
     }
     for (uint32_t e = 0; e < tsize; ++e) {
-      st[2 * (base | out_addr[e])] = tb[e].r;
-      st[2 * (base | out_addr[e]) + 1] = tb[e].i;
+      const C o = cm(sw.scale_re, sw.scale_im, tb[e]);  // the sweep's rotation-form scalar
+      st[2 * (base | out_addr[e])] = o.r;
+      st[2 * (base | out_addr[e]) + 1] = o.i;
     }
   }
 }

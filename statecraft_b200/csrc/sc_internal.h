@@ -64,9 +64,13 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        registers (a fixed register permutation).
 // SK_PAULI: Pauli slot on register bit a; b = slot, the Pauli of each trajectory
 //        comes from the sweep's choice table (0 = I, 1 = X, 2 = Y, 3 = Z).
+// SK_G1ALLQ: SK_G1ALL in rotation form: each 2x2 unitary is s_g * diag(1, e^{i phi})
+//        [[1, -t], [t, 1]] diag(1, e^{i lam}); pool per bit: t, e^{i lam}, e^{i phi}
+//        (5 reals).  The scalars s_g of a sweep multiply into SwSweep::scale, which
+//        the sweep applies to every amplitude once, when it stores the tile.
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
@@ -77,7 +81,7 @@ inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
     case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: return (kind << 4) | (a << 2);
     case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0:
       return (kind << 4) | (a << 2) | b;
-    case SK_G1ALL: return (kind << 4) | (a & 15);  // a = register-bit mask
+    case SK_G1ALL: case SK_G1ALLQ: return (kind << 4) | (a & 15);  // a = register-bit mask
     default: return kind << 4;
   }
 }
@@ -121,6 +125,7 @@ struct SwSweep {
   int32_t hs[SW_MAX_HIGH];   // the same physical bits, ascending (tile enumeration)
   int8_t outp[32];           // physical bit tile position p is written to (output layout)
   int32_t relayout;          // outp differs from the input map
+  double scale_re, scale_im;  // product of the rotation-form scalars of the sweep's gates
 };
 
 // In-place permutation of physical qubit bits: the tile is the 2^nbits
@@ -143,6 +148,9 @@ struct PlanParams {
   int max_gates;     // per sweep
   int max_pool = 1 << 30;  // matrix reals per sweep
   bool relayout = true;    // let sweeps move qubits onto the low physical bits
+  // 1-qubit unitaries with |u00| >= rot_min_c use the rotation form (0: never);
+  // the bound keeps t = |u10| / |u00| and the sweep's scalar in range
+  double rot_min_c = 0.0;
 };
 
 // matrix reals a normalised gate stores in the sweep pool

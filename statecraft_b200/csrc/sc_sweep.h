@@ -42,6 +42,8 @@ struct SweepParams {
   uint32_t gfirst[16];   // global offset of register j in the first stage's layout
   uint32_t glast[16];    // global offset register j is stored to (last stage, perm applied)
   uint16_t lastoff[16];  // tile offset register j is stored to (last stage, perm applied)
+  R scale_re, scale_im;  // applied to every amplitude at the store (rotation-form scalars)
+  int32_t has_scale, pad3;
   SwStage stages[kSweepMaxStages];
   SwStageTab tabs[kSweepMaxStages];
   SwGate gates[kSweepMaxGates];
