@@ -214,41 +214,55 @@ __device__ __forceinline__ void d1r(typename Amp<R>::type (&v)[1 << NR], const R
     v[j] = ((j >> A_) & 1) ? cmul(d1r_, d1i_, v[j]) : cmul(d0r, d0i, v[j]);
 }
 
-// rotation form on register bit A_: diag(1, e^{i phi}) [[1, -t], [t, 1]] diag(1, e^{i lam});
-// q = {t, e^{i lam}, e^{i phi}} -- 12 FP64 operations per pair instead of 16
+// Rotation form of commuting 2x2 gates on the register bits of mask M: each gate is
+// diag(1, e^{i phi}) [[1, -t], [t, 1]] diag(1, e^{i lam}) (its scalar is applied by
+// the sweep), and since the gates act on distinct bits their input and output
+// phases combine into one diagonal each.  Pool: t per bit (ascending), then the
+// input-phase table lam[s] and the output-phase table phi[s], complex, for
+// s = 1 .. 2^K - 1 (s = the bits of j in M, compacted; s = 0 is the phase 1).
+// A 4-bit record costs 15 + 15 complex multiplies and 4 x 8 rotations (248 FP64
+// operations for 16 amplitudes) where four single-bit gates cost 384.
+template <int M>
+__host__ __device__ constexpr int compact_bits(int j) {
+  int s = 0, k = 0;
+  for (int b = 0; b < 4; ++b)
+    if ((M >> b) & 1) s |= ((j >> b) & 1) << k++;
+  return s;
+}
+
 template <typename R, int NR, int A_>
-__device__ __forceinline__ void g1q(typename Amp<R>::type (&v)[1 << NR], const R* q) {
-  const R t = q[0], lr = q[1], li = q[2], pr = q[3], pi = q[4];
+__device__ __forceinline__ void rot(typename Amp<R>::type (&v)[1 << NR], const R t) {
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j) {
     if (j & (1 << A_)) continue;
     const int j1 = j | (1 << A_);
     const auto a0 = v[j], a1 = v[j1];
-    // b1 = e^{i lam} a1
-    const R b1x = fma(lr, a1.x, -li * a1.y), b1y = fma(lr, a1.y, li * a1.x);
-    // n0 = a0 - t b1, m1 = t a0 + b1, n1 = e^{i phi} m1
-    const R m1x = fma(t, a0.x, b1x), m1y = fma(t, a0.y, b1y);
-    v[j] = make_amp<R>(fma(-t, b1x, a0.x), fma(-t, b1y, a0.y));
-    v[j1] = make_amp<R>(fma(pr, m1x, -pi * m1y), fma(pr, m1y, pi * m1x));
+    v[j] = make_amp<R>(fma(-t, a1.x, a0.x), fma(-t, a1.y, a0.y));
+    v[j1] = make_amp<R>(fma(t, a0.x, a1.x), fma(t, a0.y, a1.y));
+  }
+}
+
+template <typename R, int NR, int M>
+__device__ __forceinline__ void phase_table(typename Amp<R>::type (&v)[1 << NR], const R* tab) {
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const int s = compact_bits<M>(j);
+    if (s != 0) v[j] = cmul(tab[2 * (s - 1)], tab[2 * (s - 1) + 1], v[j]);
   }
 }
 
 template <typename R, int NR, int M>
 __device__ __forceinline__ void g1allq(typename Amp<R>::type (&v)[1 << NR], const R* q) {
-  const R* qq = q;
-  if constexpr ((M & 1) != 0) {
-    g1q<R, NR, 0>(v, qq);
-    qq += 5;
-  }
-  if constexpr (NR > 1 && (M & 2) != 0) {
-    g1q<R, NR, 1>(v, qq);
-    qq += 5;
-  }
-  if constexpr (NR > 2 && (M & 4) != 0) {
-    g1q<R, NR, 2>(v, qq);
-    qq += 5;
-  }
-  if constexpr (NR > 3 && (M & 8) != 0) g1q<R, NR, 3>(v, qq);
+  constexpr int K = ((M >> 0) & 1) + ((M >> 1) & 1) + ((M >> 2) & 1) + ((M >> 3) & 1);
+  const R* lam = q + K;
+  const R* phi = lam + 2 * ((1 << K) - 1);
+  phase_table<R, NR, M>(v, lam);
+  const R* tq = q;
+  if constexpr ((M & 1) != 0) rot<R, NR, 0>(v, *tq++);
+  if constexpr (NR > 1 && (M & 2) != 0) rot<R, NR, 1>(v, *tq++);
+  if constexpr (NR > 2 && (M & 4) != 0) rot<R, NR, 2>(v, *tq++);
+  if constexpr (NR > 3 && (M & 8) != 0) rot<R, NR, 3>(v, *tq);
+  phase_table<R, NR, M>(v, phi);
 }
 
 // uncontrolled 2x2 gates on the register bits of mask M (ascending; matrices

@@ -29,7 +29,7 @@ double gate_cost(const PGate& g) {
 
 int gate_pool_size(const PGate& g) {
   switch (g.kind) {
-    case PK_DENSE1: return 8;
+    case PK_DENSE1: return 16;  // 8 as a matrix; up to 16 in a rotation-form record
     case PK_DENSE2: return 32;
     case PK_DIAG1: return 4;
     case PK_DIAG2: return 8;
@@ -652,10 +652,30 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             sr = nr;
             si = ni;
           }
+          // the stored amplitudes grow by 1 / |scalar| within the sweep: keep the
+          // plain form once the sweep's own scalar would drop below the floor
+          if (all && std::hypot(sr, si) < pp.scale_floor) all = false;
           if (all) {
             sg.kind = SK_G1ALLQ;
             for (const auto& r : run) sg.a |= 1 << r.first;
-            plan.pool.insert(plan.pool.end(), qs.begin(), qs.end());
+            // t per gate, then the input- and output-phase tables over the subsets s
+            // of the run's gates (bit k of s: gate k, in increasing register bit)
+            const int K = (int)run.size();
+            for (int k = 0; k < K; ++k) plan.pool.push_back(qs[5 * k]);
+            for (int part = 0; part < 2; ++part) {
+              for (int sub = 1; sub < (1 << K); ++sub) {
+                double pr = 1.0, pi = 0.0;
+                for (int k = 0; k < K; ++k) {
+                  if (!((sub >> k) & 1)) continue;
+                  const double er = qs[5 * k + 1 + 2 * part], ei = qs[5 * k + 2 + 2 * part];
+                  const double nr = pr * er - pi * ei, ni = pr * ei + pi * er;
+                  pr = nr;
+                  pi = ni;
+                }
+                plan.pool.push_back(pr);
+                plan.pool.push_back(pi);
+              }
+            }
             sw.scale_re = sr;
             sw.scale_im = si;
             sg.code = sw_code(sg.kind, sg.a, sg.b);
@@ -821,6 +841,27 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     while (first < G && when[first] >= 0) ++first;
   }
   plan.restore = restore_identity(phys_of, n);
+
+  // A scalar commutes with every gate, so the sweeps' rotation-form scalars need not
+  // be applied where they arise: carry their product on and apply it at the store of
+  // the last sweep, or earlier once its magnitude drops below the floor.
+  double cr = 1.0, ci = 0.0;
+  for (size_t k = 0; k < plan.sweeps.size(); ++k) {
+    SwSweep& sw = plan.sweeps[k];
+    const double nr = cr * sw.scale_re - ci * sw.scale_im;
+    const double ni = cr * sw.scale_im + ci * sw.scale_re;
+    cr = nr;
+    ci = ni;
+    if (k + 1 == plan.sweeps.size() || std::hypot(cr, ci) < pp.scale_floor) {
+      sw.scale_re = cr;
+      sw.scale_im = ci;
+      cr = 1.0;
+      ci = 0.0;
+    } else {
+      sw.scale_re = 1.0;
+      sw.scale_im = 0.0;
+    }
+  }
   return plan;
 }
 

@@ -251,8 +251,10 @@ PlanParams Ctx::plan_params() const {
   pp.max_pool = kSweepMaxPool;
   pp.relayout = relayout;
   // rotation form for 1-qubit unitaries: |u00| >= 0.05 (c128) / 0.25 (c64) keeps
-  // t <= 20 / 4 and a sweep's scalar far from under- or overflow
+  // t <= 20 / 4; the scalar floor keeps the stored amplitudes below 2^400 (c128)
+  // or 2^60 (c64), and the scalar a sweep applies a normal number
   pp.rot_min_c = rotation ? (c64 ? 0.25 : 0.05) : 0.0;
+  pp.scale_floor = c64 ? 0x1p-30 : 0x1p-200;
   return pp;
 }
 

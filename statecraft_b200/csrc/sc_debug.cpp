@@ -195,21 +195,30 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
               break;
             }
             case SK_G1ALLQ: {
-              const double* q = m;
-              for (int bit = 0; bit < NR; ++bit) {
-                if (!((g.a >> bit) & 1)) continue;
-                const double t = q[0], lr = q[1], li = q[2], pr = q[3], pi = q[4];
+              int bits[8], K = 0;
+              for (int bit = 0; bit < NR; ++bit)
+                if ((g.a >> bit) & 1) bits[K++] = bit;
+              const double* lam = m + K;
+              const double* phi = lam + 2 * ((1 << K) - 1);
+              auto subset = [&](int j) {
+                int sub = 0;
+                for (int k = 0; k < K; ++k) sub |= ((j >> bits[k]) & 1) << k;
+                return sub;
+              };
+              for (int j = 0; j < NV; ++j)
+                if (const int sub = subset(j)) v[j] = cm(lam[2 * (sub - 1)], lam[2 * (sub - 1) + 1], v[j]);
+              for (int k = 0; k < K; ++k) {
+                const double t = m[k];
                 for (int j = 0; j < NV; ++j) {
-                  if (j & (1 << bit)) continue;
-                  const int j1 = j | (1 << bit);
+                  if (j & (1 << bits[k])) continue;
+                  const int j1 = j | (1 << bits[k]);
                   const C a0 = v[j], a1 = v[j1];
-                  const C b1 = {lr * a1.r - li * a1.i, lr * a1.i + li * a1.r};
-                  const C m1 = {t * a0.r + b1.r, t * a0.i + b1.i};
-                  v[j] = {a0.r - t * b1.r, a0.i - t * b1.i};
-                  v[j1] = {pr * m1.r - pi * m1.i, pr * m1.i + pi * m1.r};
+                  v[j] = {a0.r - t * a1.r, a0.i - t * a1.i};
+                  v[j1] = {t * a0.r + a1.r, t * a0.i + a1.i};
                 }
-                q += 5;
               }
+              for (int j = 0; j < NV; ++j)
+                if (const int sub = subset(j)) v[j] = cm(phi[2 * (sub - 1)], phi[2 * (sub - 1) + 1], v[j]);
               break;
             }
             case SK_D1R:

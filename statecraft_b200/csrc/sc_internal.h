@@ -65,9 +65,11 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 // SK_PAULI: Pauli slot on register bit a; b = slot, the Pauli of each trajectory
 //        comes from the sweep's choice table (0 = I, 1 = X, 2 = Y, 3 = Z).
 // SK_G1ALLQ: SK_G1ALL in rotation form: each 2x2 unitary is s_g * diag(1, e^{i phi})
-//        [[1, -t], [t, 1]] diag(1, e^{i lam}); pool per bit: t, e^{i lam}, e^{i phi}
-//        (5 reals).  The scalars s_g of a sweep multiply into SwSweep::scale, which
-//        the sweep applies to every amplitude once, when it stores the tile.
+//        [[1, -t], [t, 1]] diag(1, e^{i lam}).  Pool: t of each of the K gates, then
+//        the products of their e^{i lam} and of their e^{i phi} over every non-empty
+//        subset of the gates (2 x (2^K - 1) complex; bit k of the subset index is the
+//        k-th gate in increasing register bit).  The scalars s_g are carried in
+//        SwSweep::scale and applied to every amplitude at a sweep's store.
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
   SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ
@@ -125,7 +127,9 @@ struct SwSweep {
   int32_t hs[SW_MAX_HIGH];   // the same physical bits, ascending (tile enumeration)
   int8_t outp[32];           // physical bit tile position p is written to (output layout)
   int32_t relayout;          // outp differs from the input map
-  double scale_re, scale_im;  // product of the rotation-form scalars of the sweep's gates
+  // the rotation-form scalar this sweep applies at its store: the product of its own
+  // gates' scalars and those carried from earlier sweeps (1 when it carries them on)
+  double scale_re, scale_im;
 };
 
 // In-place permutation of physical qubit bits: the tile is the 2^nbits
@@ -149,8 +153,12 @@ struct PlanParams {
   int max_pool = 1 << 30;  // matrix reals per sweep
   bool relayout = true;    // let sweeps move qubits onto the low physical bits
   // 1-qubit unitaries with |u00| >= rot_min_c use the rotation form (0: never);
-  // the bound keeps t = |u10| / |u00| and the sweep's scalar in range
+  // the bound keeps t = |u10| / |u00| in range
   double rot_min_c = 0.0;
+  // smallest magnitude of the rotation-form scalar, both the part a sweep collects
+  // and the part carried from earlier sweeps: the stored amplitudes are the true
+  // ones divided by the scalar, so they stay below 1 / scale_floor^2
+  double scale_floor = 0x1p-200;
 };
 
 // matrix reals a normalised gate stores in the sweep pool

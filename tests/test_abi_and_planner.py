@@ -176,3 +176,28 @@ def test_relayout_reduces_sweeps(monkeypatch):
     _, without = _plan_info(c, 10, 4, 3, -1.0)
     assert without["relayouts"] == 0 and without["restores"] == 0
     assert with_layout["sweeps"] < 0.8 * without["sweeps"]
+
+
+def test_rotation_form_scalar_stays_in_range():
+    # 1-qubit gates in rotation form leave a scalar |u00| per gate that the sweeps
+    # apply late; a long chain of near-pi rotations (|u00| = 0.06, just above the
+    # 0.05 bound) would push the stored amplitudes past the double range without
+    # the floor on that scalar
+    from statecraft_b200 import quantum as Q
+
+    n = 10
+    theta = 2 * np.arccos(0.06)
+    c = Q.QuantumCircuit(n)
+    for q in range(n):
+        c = c.append(Q.Hadamard(), q)
+    rng = np.random.default_rng(6)
+    for _ in range(400):
+        q = int(rng.integers(0, n))
+        c = c.append(Q.u3(theta, float(rng.uniform(0, 6.3)), float(rng.uniform(0, 6.3))), q)
+        if rng.random() < 0.1:
+            c = c.append(Q.CnotGate.of(), q, (q + 1) % n)
+    init = RCirc.random_state(n, 3)
+    for cfg in [(6, 2, 2, -1.0), (8, 3, 3, -1.0), (11, 4, 4, -1.0)]:
+        got, _ = _emulate(c, init, *cfg)
+        assert np.all(np.isfinite(got))
+        np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)

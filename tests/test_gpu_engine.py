@@ -263,6 +263,37 @@ def test_complex64_error_vs_complex128(n, c64):
     assert np.max(np.abs(got - want)) < 2e-5
 
 
+def _near_pi_chain(n, u00, gates, seed):
+    # H on every qubit, then a long chain of u3 gates with |u00| = u00 (and a few
+    # CNOTs): the rotation-form scalars of the chain multiply to far below the
+    # floating-point range unless the sweeps apply them in time
+    c = Q.QuantumCircuit(n)
+    for q in range(n):
+        c = c.append(Q.Hadamard(), q)
+    rng = np.random.default_rng(seed)
+    theta = 2 * math.acos(u00)
+    for _ in range(gates):
+        q = int(rng.integers(0, n))
+        c = c.append(Q.u3(theta, float(rng.uniform(0, 6.3)), float(rng.uniform(0, 6.3))), q)
+        if rng.random() < 0.1:
+            c = c.append(Q.CnotGate.of(), q, (q + 1) % n)
+    return c
+
+
+@pytest.mark.parametrize("n", [12, 20])
+def test_rotation_form_scalar_stays_in_range(n, fused, c64):
+    c = _near_pi_chain(n, 0.06, 600, n)
+    want = _oracle_state(c)
+    got = fused.simulate(SimulationRequest.zeroState(c)).finalState.data()
+    assert np.all(np.isfinite(got))
+    np.testing.assert_allclose(got, want, rtol=0, atol=EPS)
+    c = _near_pi_chain(n, 0.26, 600, n + 1)
+    want = _oracle_state(c)
+    got = c64.simulate(SimulationRequest.zeroState(c)).finalState.data()
+    assert np.all(np.isfinite(got))
+    assert np.max(np.abs(got - want)) < 2e-5
+
+
 # ---- expectation values / adjoint ---------------------------------------------
 def test_pauli_expectation_matches_oracle(fused):
     n = 10
