@@ -627,83 +627,84 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       // runs of uncontrolled 2x2 gates on distinct register bits become one record
       std::vector<std::pair<int, const double*>> run;
       std::vector<int64_t> run_ops;
-      auto flush_run = [&]() {
-        if (run.empty()) return;
+      // rotation-form record for the gates of `part` (increasing register bit)
+      auto emit_rotation = [&](const std::vector<int>& part, const std::vector<double>& qs) {
         SwGate sg;
         std::memset(&sg, 0, sizeof sg);
         sg.moff = (int32_t)plan.pool.size();
-        // rotation form when every gate of the run has one
-        {
-          std::sort(run.begin(), run.end(),
-                    [](const std::pair<int, const double*>& x, const std::pair<int, const double*>& y) {
-                      return x.first < y.first;
-                    });
-          std::vector<double> qs;
-          double sr = sw.scale_re, si = sw.scale_im;
-          bool all = true;
-          for (const auto& r : run) {
-            double q[5], fr, fi;
-            if (!rotation_form(r.second, pp.rot_min_c, q, &fr, &fi)) {
-              all = false;
-              break;
+        sg.kind = SK_G1ALLQ;
+        for (int i : part) sg.a |= 1 << run[i].first;
+        // t per gate, then the input- and output-phase tables over the subsets s of
+        // the record's gates (bit k of s: gate k, in increasing register bit)
+        const int K = (int)part.size();
+        for (int k = 0; k < K; ++k) plan.pool.push_back(qs[5 * k]);
+        for (int side = 0; side < 2; ++side) {
+          for (int sub = 1; sub < (1 << K); ++sub) {
+            double pr = 1.0, pi = 0.0;
+            for (int k = 0; k < K; ++k) {
+              if (!((sub >> k) & 1)) continue;
+              const double er = qs[5 * k + 1 + 2 * side], ei = qs[5 * k + 2 + 2 * side];
+              const double nr = pr * er - pi * ei, ni = pr * ei + pi * er;
+              pr = nr;
+              pi = ni;
             }
-            qs.insert(qs.end(), q, q + 5);
-            const double nr = sr * fr - si * fi, ni = sr * fi + si * fr;
-            sr = nr;
-            si = ni;
-          }
-          // the stored amplitudes grow by 1 / |scalar| within the sweep: keep the
-          // plain form once the sweep's own scalar would drop below the floor
-          if (all && std::hypot(sr, si) < pp.scale_floor) all = false;
-          if (all) {
-            sg.kind = SK_G1ALLQ;
-            for (const auto& r : run) sg.a |= 1 << r.first;
-            // t per gate, then the input- and output-phase tables over the subsets s
-            // of the run's gates (bit k of s: gate k, in increasing register bit)
-            const int K = (int)run.size();
-            for (int k = 0; k < K; ++k) plan.pool.push_back(qs[5 * k]);
-            for (int part = 0; part < 2; ++part) {
-              for (int sub = 1; sub < (1 << K); ++sub) {
-                double pr = 1.0, pi = 0.0;
-                for (int k = 0; k < K; ++k) {
-                  if (!((sub >> k) & 1)) continue;
-                  const double er = qs[5 * k + 1 + 2 * part], ei = qs[5 * k + 2 + 2 * part];
-                  const double nr = pr * er - pi * ei, ni = pr * ei + pi * er;
-                  pr = nr;
-                  pi = ni;
-                }
-                plan.pool.push_back(pr);
-                plan.pool.push_back(pi);
-              }
-            }
-            sw.scale_re = sr;
-            sw.scale_im = si;
-            sg.code = sw_code(sg.kind, sg.a, sg.b);
-            plan.gates.push_back(sg);
-            plan.gate_ops.insert(plan.gate_ops.end(), run_ops.begin(), run_ops.end());
-            run.clear();
-            run_ops.clear();
-            return;
-          }
-        }
-        if (run.size() == 1) {
-          sg.kind = SK_G1;
-          sg.a = run[0].first;
-          plan.pool.insert(plan.pool.end(), run[0].second, run[0].second + 8);
-        } else {
-          std::sort(run.begin(), run.end(),
-                    [](const std::pair<int, const double*>& x, const std::pair<int, const double*>& y) {
-                      return x.first < y.first;
-                    });
-          sg.kind = SK_G1ALL;
-          for (const auto& r : run) {
-            sg.a |= 1 << r.first;
-            plan.pool.insert(plan.pool.end(), r.second, r.second + 8);
+            plan.pool.push_back(pr);
+            plan.pool.push_back(pi);
           }
         }
         sg.code = sw_code(sg.kind, sg.a, sg.b);
         plan.gates.push_back(sg);
-        plan.gate_ops.insert(plan.gate_ops.end(), run_ops.begin(), run_ops.end());
+        for (int i : part) plan.gate_ops.push_back(run_ops[i]);
+      };
+      // matrix record (G1 or G1ALL) for the gates of `part` (increasing register bit)
+      auto emit_matrix = [&](const std::vector<int>& part) {
+        SwGate sg;
+        std::memset(&sg, 0, sizeof sg);
+        sg.moff = (int32_t)plan.pool.size();
+        if (part.size() == 1) {
+          sg.kind = SK_G1;
+          sg.a = run[part[0]].first;
+        } else {
+          sg.kind = SK_G1ALL;
+          for (int i : part) sg.a |= 1 << run[i].first;
+        }
+        for (int i : part) plan.pool.insert(plan.pool.end(), run[i].second, run[i].second + 8);
+        sg.code = sw_code(sg.kind, sg.a, sg.b);
+        plan.gates.push_back(sg);
+        for (int i : part) plan.gate_ops.push_back(run_ops[i]);
+      };
+      // The run's gates act on distinct register bits and commute: those with a
+      // rotation form make one rotation-form record, the others one matrix record.
+      auto flush_run = [&]() {
+        if (run.empty()) return;
+        std::vector<int> order(run.size());
+        for (size_t i = 0; i < run.size(); ++i) order[i] = (int)i;
+        std::sort(order.begin(), order.end(), [&](int x, int y) { return run[x].first < run[y].first; });
+        std::vector<int> rot, mat;
+        std::vector<double> qs;
+        double sr = sw.scale_re, si = sw.scale_im;
+        for (int i : order) {
+          double q[5], fr, fi;
+          bool ok = rotation_form(run[i].second, pp.rot_min_c, q, &fr, &fi);
+          const double nr = sr * fr - si * fi, ni = sr * fi + si * fr;
+          // the stored amplitudes grow by 1 / |scalar| within the sweep: keep the
+          // matrix form once the sweep's own scalar would drop below the floor
+          if (ok && std::hypot(nr, ni) < pp.scale_floor) ok = false;
+          if (ok) {
+            rot.push_back(i);
+            qs.insert(qs.end(), q, q + 5);
+            sr = nr;
+            si = ni;
+          } else {
+            mat.push_back(i);
+          }
+        }
+        if (!rot.empty()) {
+          emit_rotation(rot, qs);
+          sw.scale_re = sr;
+          sw.scale_im = si;
+        }
+        if (!mat.empty()) emit_matrix(mat);
         run.clear();
         run_ops.clear();
       };

@@ -201,3 +201,24 @@ def test_rotation_form_scalar_stays_in_range():
         got, _ = _emulate(c, init, *cfg)
         assert np.all(np.isfinite(got))
         np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
+
+
+def test_runs_mixing_rotation_and_matrix_gates():
+    # layers of u3 gates where some have |u00| below the rotation-form bound (0.05):
+    # a run of commuting gates splits into a rotation-form record and a matrix record
+    from statecraft_b200 import quantum as Q
+
+    n = 12
+    rng = np.random.default_rng(12)
+    c = Q.QuantumCircuit(n)
+    for layer in range(8):
+        for q in range(n):
+            u00 = 0.01 if rng.random() < 0.3 else float(rng.uniform(0.1, 1.0))
+            c = c.append(Q.u3(2 * np.arccos(u00), float(rng.uniform(0, 6.3)),
+                              float(rng.uniform(0, 6.3))), q)
+        for q in range(layer % 2, n - 1, 2):
+            c = c.append(Q.CnotGate.of(), q, q + 1)
+    init = RCirc.random_state(n, 5)
+    for cfg in [(11, 4, 4, -1.0), (8, 3, 3, -1.0), (6, 2, 2, -1.0)]:
+        got, _ = _emulate(c, init, *cfg)
+        np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
