@@ -193,6 +193,24 @@ __device__ __forceinline__ void xswap0(typename Amp<R>::type (&v)[1 << NR]) {
   }
 }
 
+// X on register bit A_ applied to the stage's exit slots: the amplitude in register
+// j leaves through the slot of register j ^ (1 << A_), whose swizzled offset differs
+// by m = soff[1 << A_] (the offsets are linear in j); m = 0 where the gate's
+// controls outside the registers are not all set
+template <int NR, int A_>
+__device__ __forceinline__ void xfold(uint32_t (&sidx)[1 << NR], uint32_t m) {
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) sidx[j] ^= m;
+}
+
+// the same for X on register bit T_ controlled by register bit C_
+template <int NR, int T_, int C_>
+__device__ __forceinline__ void cxfold(uint32_t (&sidx)[1 << NR], uint32_t m) {
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j)
+    if (j & (1 << C_)) sidx[j] ^= m;
+}
+
 // controlled X, target register bit T_, control register bit C_, no other tile controls
 template <typename R, int NR, int T_, int C_>
 __device__ __forceinline__ void cxswap0(typename Amp<R>::type (&v)[1 << NR]) {
@@ -581,8 +599,16 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   if constexpr (kBatch) {                     \
     pauli<R, NR, A>(v, (uint32_t)codes[g.b]); \
   }
+#define SC_DO_XF(A) \
+  xfold<NR, A>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.soff[1 << (A)] : 0u)
+#define SC_DO_CXF(A, B) \
+  cxfold<NR, A, B>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.soff[1 << (A)] : 0u)
           SC_CASES_1(SK_X0, SC_DO_X0)
           SC_CASES_2(SK_CX0, SC_DO_CX0)
+          SC_CASES_1(SK_XF, SC_DO_XF)
+          SC_CASES_2(SK_CXF, SC_DO_CXF)
+#undef SC_DO_XF
+#undef SC_DO_CXF
           SC_CASES_1(SK_PAULI, SC_DO_PAULI)
 #undef SC_DO_X0
 #undef SC_DO_CX0
@@ -844,6 +870,9 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
       p->tabs[s].wsoff[j] = p->tabs[s].soff[pj];
     }
   }
+  // slot folds act on the exchange slots: none may sit in the last stage
+  for (int g = plan.stages[sw.s1 - 1].g0; g < plan.stages[sw.s1 - 1].g1; ++g)
+    if (plan.gates[g].kind == SK_XF || plan.gates[g].kind == SK_CXF) return false;
   const SwStage& last = p->stages[ns - 1];
   for (int j = 0; j < 16; ++j) {
     const int pj = (j < nv) ? last.perm[j] : j;
@@ -851,9 +880,12 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
     p->lastoff[j] = p->tabs[ns - 1].off[pj];
     p->glast[j] = host_spread_out(p->lastoff[j], sw);
   }
-  const int32_t pool_lo = (g_hi > g_lo) ? plan.gates[g_lo].moff : 0;
+  // the sweep's record data: the pool entries appended while it was planned (records
+  // need not reference them in order: the stage peephole moves records)
+  const int32_t pool_lo = sw.pool0, pool_hi = sw.pool1;
   for (int g = g_lo; g < g_hi; ++g) {
     SwGate sg = plan.gates[g];
+    if (sg.moff < pool_lo || sg.moff > pool_hi) return false;
     sg.moff -= pool_lo;
     if (sg.kind == SK_PAULI) {  // slot -> local index into the staged choices
       if (p->n_local_slots >= kSweepMaxGates) return false;
@@ -862,13 +894,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
     }
     p->gates[g - g_lo] = sg;
   }
-  // the pool slice of this sweep ends where the next sweep's first gate begins
-  int32_t pool_hi = (int32_t)plan.pool.size();
-  if (k + 1 < plan.sweeps.size()) {
-    const int next_g = plan.stages[plan.sweeps[k + 1].s0].g0;
-    if (next_g < (int)plan.gates.size()) pool_hi = plan.gates[next_g].moff;
-  }
-  if (pool_hi - pool_lo > kSweepMaxPool) return false;
+  if (pool_hi < pool_lo || pool_hi - pool_lo > kSweepMaxPool) return false;
   for (int32_t e = pool_lo; e < pool_hi; ++e) p->pool[e - pool_lo] = (R)plan.pool[e];
   p->pool_len = pool_hi - pool_lo;
   return true;

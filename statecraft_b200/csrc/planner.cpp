@@ -244,6 +244,219 @@ bool rotation_form(const double* u, double min_c, double* q, double* fr, double*
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Stage peephole: fewer records per stage.  Every record costs a dispatch and a
+// reconciliation of the register-resident amplitudes, so register-bit diagonals
+// are moved towards the start of the stage (conjugated through plain register
+// permutations: d'(x) = d(P x) for an involution P), merged into the phase table of
+// a rotation-form record that covers their bits, and plain permutations that end
+// up last to touch their bits are folded into the stage's exit permutation.
+// ---------------------------------------------------------------------------
+namespace {
+
+bool sk_diagonal(int32_t k) {
+  return k == SK_D1 || k == SK_D2 || k == SK_DP || k == SK_D1R || k == SK_DPR;
+}
+
+// register bits a record reads or writes (tile positions mapped through reg_of_pos)
+uint32_t record_bits(const SwGate& g, const int* reg_of_pos) {
+  uint32_t f = 0;
+  auto reg = [&](int p) {
+    if (p >= 0 && p < 32 && reg_of_pos[p] >= 0) f |= 1u << reg_of_pos[p];
+  };
+  switch (g.kind) {
+    case SK_G1: case SK_X: case SK_X0: case SK_D1R: case SK_PAULI: case SK_XF: f |= 1u << g.a; break;
+    case SK_G2: case SK_CX: case SK_CX0: case SK_DPR: case SK_SWAP: case SK_CXF:
+      f |= (1u << g.a) | (1u << g.b);
+      break;
+    case SK_G1ALL: case SK_G1ALLQ: f |= (uint32_t)g.a & 15u; break;
+    case SK_D1: reg(g.a); break;
+    case SK_DP: case SK_D2: reg(g.a); reg(g.b); break;
+    default: return 0xFFFFFFFFu;
+  }
+  for (uint32_t m = g.lmask; m; m &= m - 1) reg(__builtin_ctz(m));
+  return f;
+}
+
+// X / CX / SWAP on register bits with no tile or global controls
+bool plain_permutation(const SwGate& g) {
+  return (g.kind == SK_X0 || g.kind == SK_CX0 || g.kind == SK_SWAP) && g.gmask == 0 && g.lmask == 0;
+}
+
+// register bits a plain permutation changes (a SWAP's both, an X's target)
+uint32_t written_bits(const SwGate& p) {
+  return p.kind == SK_SWAP ? (1u << p.a) | (1u << p.b) : 1u << p.a;
+}
+
+// X / CX on register bits whose other controls lie outside the registers
+bool conditional_permutation(const SwGate& g, const int* reg_of_pos) {
+  if (g.kind == SK_X0 || g.kind == SK_X) return record_bits(g, reg_of_pos) == 1u << g.a;
+  if (g.kind == SK_CX0 || g.kind == SK_CX)
+    return record_bits(g, reg_of_pos) == ((1u << g.a) | (1u << g.b));
+  return false;
+}
+
+bool register_diagonal(const SwGate& g) {
+  return (g.kind == SK_D1R || g.kind == SK_DPR) && g.gmask == 0 && g.lmask == 0;
+}
+
+// entry of a D1R / DPR record (pool: two complex values) at register index x
+void diagonal_at(const SwGate& d, const std::vector<double>& pool, int x, double* re, double* im) {
+  const int k = d.kind == SK_D1R ? (x >> d.a) & 1 : ((x >> d.a) ^ (x >> d.b)) & 1;
+  *re = pool[d.moff + 2 * k];
+  *im = pool[d.moff + 2 * k + 1];
+}
+
+// Rewrites diagonal d (applied after plain permutation p) as the diagonal to apply
+// before p; false when the result is not a D1R / DPR record.
+bool conjugate_diagonal(SwGate& d, const SwGate& p, std::vector<double>& pool) {
+  const uint32_t db = d.kind == SK_D1R ? 1u << d.a : (1u << d.a) | (1u << d.b);
+  auto set = [&](int32_t kind, int32_t a, int32_t b) {
+    d.kind = kind;
+    d.a = a;
+    d.b = b;
+    d.code = sw_code(kind, a, b);
+  };
+  if (p.kind == SK_X0) {  // d(x ^ e_a): the entries trade places when a is one of d's bits
+    if ((db >> p.a) & 1) {
+      std::swap(pool[d.moff], pool[d.moff + 2]);
+      std::swap(pool[d.moff + 1], pool[d.moff + 3]);
+    }
+    return true;
+  }
+  if (p.kind == SK_SWAP) {
+    auto map = [&](int32_t b) { return b == p.a ? p.b : (b == p.b ? p.a : b); };
+    if (d.kind == SK_D1R) set(SK_D1R, map(d.a), 0);
+    else set(SK_DPR, map(d.a), map(d.b));
+    return true;
+  }
+  if (p.kind == SK_CX0) {  // target p.a, control p.b: x_t -> x_t ^ x_c
+    const int32_t t = p.a, c = p.b;
+    if (!((db >> t) & 1)) return true;
+    if (d.kind == SK_D1R) {  // d(x_t ^ x_c): a parity diagonal on (t, c)
+      set(SK_DPR, t, c);
+      return true;
+    }
+    const int32_t o = d.a == t ? d.b : d.a;
+    if (o == c) {  // parity of (x_t ^ x_c, x_c) is x_t
+      set(SK_D1R, t, 0);
+      return true;
+    }
+  }
+  return false;
+}
+
+// Merges unitary diagonal d into the output (after) or input (before) phase table of
+// rotation-form record g when d's bits are among g's; d(0) joins the sweep scalar.
+bool merge_diagonal(const SwGate& g, const SwGate& d, bool after, std::vector<double>& pool,
+                    double* sr, double* si) {
+  const uint32_t M = (uint32_t)g.a & 15u;
+  const uint32_t db = d.kind == SK_D1R ? 1u << d.a : (1u << d.a) | (1u << d.b);
+  if (g.kind != SK_G1ALLQ || g.gmask || g.lmask || (db & ~M)) return false;
+  int bits[4], K = 0;
+  for (int b = 0; b < 4; ++b)
+    if ((M >> b) & 1) bits[K++] = b;
+  double e[4];
+  for (int k = 0; k < 2; ++k) {
+    e[2 * k] = pool[d.moff + 2 * k];
+    e[2 * k + 1] = pool[d.moff + 2 * k + 1];
+    if (std::fabs(e[2 * k] * e[2 * k] + e[2 * k + 1] * e[2 * k + 1] - 1.0) > 1e-12) return false;
+  }
+  double d0r, d0i;
+  diagonal_at(d, pool, 0, &d0r, &d0i);
+  const int base = g.moff + K + (after ? 2 * ((1 << K) - 1) : 0);
+  for (int s = 1; s < (1 << K); ++s) {
+    int x = 0;
+    for (int k = 0; k < K; ++k)
+      if ((s >> k) & 1) x |= 1 << bits[k];
+    double dr, di;
+    diagonal_at(d, pool, x, &dr, &di);
+    const double rr = dr * d0r + di * d0i, ri = di * d0r - dr * d0i;  // d(x) / d(0)
+    double& tr = pool[base + 2 * (s - 1)];
+    double& ti = pool[base + 2 * (s - 1) + 1];
+    const double nr = tr * rr - ti * ri, ni = tr * ri + ti * rr;
+    tr = nr;
+    ti = ni;
+  }
+  const double nr = *sr * d0r - *si * d0i, ni = *sr * d0i + *si * d0r;
+  *sr = nr;
+  *si = ni;
+  return true;
+}
+
+// exit permutation of a stage after plain permutation p (applied at the end)
+void compose_permutation(SwStage& st, const SwGate& p) {
+  for (int j = 0; j < 16; ++j) {
+    int x = st.perm[j];
+    if (p.kind == SK_SWAP) {
+      if (((x >> p.a) ^ (x >> p.b)) & 1) x ^= (1 << p.a) | (1 << p.b);
+    } else if (p.kind == SK_X0) {
+      x ^= 1 << p.a;
+    } else if ((x >> p.b) & 1) {
+      x ^= 1 << p.a;
+    }
+    st.perm[j] = (int8_t)x;
+  }
+}
+
+// folded_bits: register bits of the permutations folded while the stage was built;
+// last: the sweep's last stage (its exit is the global store: no slot folds)
+void optimize_stage(Plan& plan, int32_t g0, SwStage& st, const int* reg_of_pos,
+                    uint32_t folded_bits, bool last, double* sr, double* si) {
+  std::vector<SwGate>& G = plan.gates;
+  for (int i = g0; i < (int)G.size(); ++i) {
+    if (!sk_diagonal(G[i].kind)) continue;
+    const bool reg_diag = register_diagonal(G[i]);
+    int j = i;
+    bool merged = false;
+    while (j > g0) {
+      const SwGate& p = G[j - 1];
+      if (reg_diag && merge_diagonal(p, G[j], true, plan.pool, sr, si)) {
+        merged = true;
+        break;
+      }
+      const uint32_t df = record_bits(G[j], reg_of_pos);
+      if (sk_diagonal(p.kind) || !(record_bits(p, reg_of_pos) & df) ||
+          (plain_permutation(p) && !(written_bits(p) & df))) {
+        std::swap(G[j - 1], G[j]);
+        --j;
+        continue;
+      }
+      if (reg_diag && plain_permutation(p)) {
+        SwGate d = G[j];
+        if (conjugate_diagonal(d, p, plan.pool)) {
+          G[j] = p;
+          G[j - 1] = d;
+          --j;
+          continue;
+        }
+      }
+      break;
+    }
+    if (merged) {
+      G.erase(G.begin() + j);
+      --i;
+    }
+  }
+  uint32_t later = folded_bits;
+  for (int k = (int)G.size() - 1; k >= g0; --k) {
+    SwGate& g = G[k];
+    const uint32_t f = record_bits(g, reg_of_pos);
+    if (!(f & later)) {
+      if (plain_permutation(g)) {
+        compose_permutation(st, g);
+        G.erase(G.begin() + k);
+      } else if (!last && conditional_permutation(g, reg_of_pos)) {
+        g.kind = (g.kind == SK_X0 || g.kind == SK_X) ? SK_XF : SK_CXF;
+        g.code = sw_code(g.kind, g.a, g.b);
+      }
+    }
+    later |= f;
+  }
+}
+
+}  // namespace
+
 // In-place bit permutations that take the layout phys_of back to the identity:
 // transpositions of physical bits, grouped while their bits (plus the low bits,
 // which keep the copies coalesced) fit one permutation tile.
@@ -495,6 +708,7 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
     staged.assign(list.size(), 0);
     size_t remaining = list.size();
     sw.s0 = (int32_t)plan.stages.size();
+    sw.pool0 = (int32_t)plan.pool.size();
     std::vector<std::pair<uint32_t, std::vector<int32_t>>> stage_list;
     // folded[i]: list gate i is a permutation folded into its stage's exit permutation
     std::vector<char> folded(list.size(), 0);
@@ -624,6 +838,7 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       st.g0 = (int32_t)plan.gates.size();
       for (int j = 0; j < 16; ++j) st.perm[j] = (int8_t)j;
       std::vector<int64_t> folded_ops;
+      uint32_t folded_bits = 0;
       // runs of uncontrolled 2x2 gates on distinct register bits become one record
       std::vector<std::pair<int, const double*>> run;
       std::vector<int64_t> run_ops;
@@ -726,6 +941,9 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             }
             st.perm[j] = (int8_t)x;
           }
+          folded_bits |= 1u << ta;
+          if (cb >= 0) folded_bits |= 1u << cb;
+          if (sb >= 0) folded_bits |= 1u << sb;
           folded_ops.push_back(pg.op_index);
           continue;
         }
@@ -824,11 +1042,15 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         plan.gate_ops.push_back(pg.op_index);
       }
       flush_run();
+      if (pp.peephole)
+        optimize_stage(plan, st.g0, st, reg_of_pos, folded_bits, is_last, &sw.scale_re,
+                       &sw.scale_im);
       plan.gate_ops.insert(plan.gate_ops.end(), folded_ops.begin(), folded_ops.end());
       st.g1 = (int32_t)plan.gates.size();
       plan.stages.push_back(st);
     }
     sw.s1 = (int32_t)plan.stages.size();
+    sw.pool1 = (int32_t)plan.pool.size();
     plan.sweeps.push_back(sw);
     // the layout after this sweep
     for (int p = 0; p < T; ++p) {

@@ -255,6 +255,7 @@ PlanParams Ctx::plan_params() const {
   // or 2^60 (c64), and the scalar a sweep applies a normal number
   pp.rot_min_c = rotation ? (c64 ? 0.25 : 0.05) : 0.0;
   pp.scale_floor = c64 ? 0x1p-30 : 0x1p-200;
+  pp.peephole = peephole;
   return pp;
 }
 
@@ -469,6 +470,7 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
   if (const char* v = getenv("STATECRAFT_B200_NR")) c->nr = atoi(v);
   if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) c->relayout = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_ROTATION")) c->rotation = atoi(v) != 0;
+  if (const char* v = getenv("STATECRAFT_B200_PEEPHOLE")) c->peephole = atoi(v) != 0;
   *out_ctx = c;
   return SC_OK;
 }

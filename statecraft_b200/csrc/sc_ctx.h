@@ -39,6 +39,7 @@ struct Ctx {
   int nr = 0;
   bool relayout = true;
   bool rotation = true;  // rotation form for 1-qubit unitaries in sweeps
+  bool peephole = true;  // per-stage record peephole in the planner
 
   // state
   int n = 0;

@@ -29,6 +29,7 @@ PlanParams debug_params(int tile, int low, int nr, double budget) {
   if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) pp.relayout = atoi(v) != 0;
   pp.rot_min_c = 0.05;
   if (const char* v = getenv("STATECRAFT_B200_ROTATION")) pp.rot_min_c = atoi(v) != 0 ? 0.05 : 0.0;
+  if (const char* v = getenv("STATECRAFT_B200_PEEPHOLE")) pp.peephole = atoi(v) != 0;
   return pp;
 }
 
@@ -80,6 +81,12 @@ inline C mac2(const double* m0, C a0, const double* m1, C a1) {
 // at position l0 | off[perm[j]]), and the tile is scattered through the output
 // layout -- the kernel's shared-memory tile, exchanges and final store.
 void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
+  // the kernel sees only the sweep's pool range: a record outside it poisons the state
+  for (int gi = plan.stages[sw.s0].g0; gi < plan.stages[sw.s1 - 1].g1; ++gi)
+    if (plan.gates[gi].moff < sw.pool0 || plan.gates[gi].moff > sw.pool1) {
+      for (uint64_t e = 0; e < 2ULL * (uint64_t)sw.tiles << sw.T; ++e) st[e] = std::nan("");
+      return;
+    }
   const int NR = sw.nr, NV = 1 << NR;
   const uint32_t tsize = 1u << sw.T;
   const uint32_t threads = 1u << (sw.T - NR);
@@ -106,6 +113,7 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
           const int b = stg.R[k];
           l0 = ((l0 >> b) << (b + 1)) | (l0 & ((1u << b) - 1u));
         }
+        uint32_t xo[16] = {0};  // slot folds: tile-index flips of each register's exit
         for (int j = 0; j < NV; ++j) {
           uint32_t o = 0;
           for (int k = 0; k < NR; ++k)
@@ -119,6 +127,12 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
           const double* m = plan.pool.data() + g.moff;
           auto ok = [&](int j) { return ((l0 | off[j]) & g.lmask) == g.lmask; };
           switch (g.kind) {
+            case SK_XF:
+            case SK_CXF:
+              if ((l0 & g.lmask) == g.lmask)
+                for (int j = 0; j < NV; ++j)
+                  if (g.kind == SK_XF || (j & (1 << g.b))) xo[j] ^= 1u << stg.R[g.a];
+              break;
             case SK_X0:
               for (int j = 0; j < NV; ++j)
                 if (!(j & (1 << g.a))) std::swap(v[j], v[j | (1 << g.a)]);
@@ -250,7 +264,7 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
           }
         }
         // folded permutations: register j leaves the stage as register perm[j]
-        for (int j = 0; j < NV; ++j) tb[l0 | off[stg.perm[j]]] = v[j];
+        for (int j = 0; j < NV; ++j) tb[(l0 | off[stg.perm[j]]) ^ xo[j]] = v[j];
       }
     }
     for (uint32_t e = 0; e < tsize; ++e) {

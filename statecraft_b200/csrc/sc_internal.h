@@ -70,9 +70,13 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        subset of the gates (2 x (2^K - 1) complex; bit k of the subset index is the
 //        k-th gate in increasing register bit).  The scalars s_g are carried in
 //        SwSweep::scale and applied to every amplitude at a sweep's store.
+// SK_XF / SK_CXF: X on register bit a (controlled by register bit b for CXF) whose
+//        other controls lie outside the registers (lmask: tile positions, gmask:
+//        global qubits), last to touch its bits in a stage that is not the sweep's
+//        last: applied to the stage's exit slots instead of the registers.
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
@@ -80,8 +84,9 @@ enum SwKind : int32_t {
 // kernel switches on it once.
 inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
   switch (kind) {
-    case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: return (kind << 4) | (a << 2);
-    case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0:
+    case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: case SK_XF:
+      return (kind << 4) | (a << 2);
+    case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0: case SK_CXF:
       return (kind << 4) | (a << 2) | b;
     case SK_G1ALL: case SK_G1ALLQ: return (kind << 4) | (a & 15);  // a = register-bit mask
     default: return kind << 4;
@@ -122,6 +127,7 @@ struct SwStage {    // 32 bytes
 struct SwSweep {
   int32_t T, L, h, nr;
   int32_t s0, s1;            // stage range
+  int32_t pool0, pool1;      // range of plan.pool holding this sweep's record data
   int64_t tiles;
   int32_t hq[SW_MAX_HIGH];   // physical bit of tile position L + k (input layout)
   int32_t hs[SW_MAX_HIGH];   // the same physical bits, ascending (tile enumeration)
@@ -159,6 +165,8 @@ struct PlanParams {
   // and the part carried from earlier sweeps: the stored amplitudes are the true
   // ones divided by the scalar, so they stay below 1 / scale_floor^2
   double scale_floor = 0x1p-200;
+  // per-stage record peephole (diagonals merged or moved, permutations folded)
+  bool peephole = true;
 };
 
 // matrix reals a normalised gate stores in the sweep pool

@@ -222,3 +222,18 @@ def test_runs_mixing_rotation_and_matrix_gates():
     for cfg in [(11, 4, 4, -1.0), (8, 3, 3, -1.0), (6, 2, 2, -1.0)]:
         got, _ = _emulate(c, init, *cfg)
         np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("peephole", ["1", "0"])
+@pytest.mark.parametrize("cfg", [(11, 4, 4, -1.0), (10, 4, 3, -1.0), (9, 3, 3, -1.0)])
+def test_stage_peephole_matches_oracle(cfg, peephole, monkeypatch):
+    # brick-wall layers with a multi-controlled Z and RZZ (the headline structure):
+    # CNOTs with controls outside the registers become exit-slot folds, diagonals
+    # move through register permutations and merge into rotation tables
+    from statecraft_b200 import workloads as W
+
+    monkeypatch.setenv("STATECRAFT_B200_PEEPHOLE", peephole)
+    c = W.brickwall_circuit(17, 5, seed=1717, mcz=True, rzz=True)
+    init = RCirc.random_state(17, 17)
+    got, _ = _emulate(c, init, *cfg)
+    np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
