@@ -161,6 +161,59 @@ __device__ __forceinline__ void rswap(typename Amp<R>::type (&v)[1 << NR]) {
   }
 }
 
+// Diagonals whose bits may lie outside the registers: a tile position (ref >= 0,
+// read from the thread's tile index) or a global qubit (ref < 0, fixed per tile).
+// diag1: diag(d0, d1) on one bit with tile-position controls lmask.
+template <typename R, int NR>
+__device__ __forceinline__ void diag1_any(typename Amp<R>::type (&v)[1 << NR], const R* m, int a,
+                                          uint32_t l0, const uint32_t (&off)[1 << NR],
+                                          uint32_t lmask, uint32_t base) {
+  const uint32_t gb = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
+  const int sh = a < 0 ? 0 : a;
+  const uint32_t lm = a < 0 ? 0u : 1u;
+  const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const uint32_t li = l0 | off[j];
+    if ((li & lmask) != lmask) continue;
+    const uint32_t bit = ((li >> sh) & lm) | gb;
+    v[j] = cmul(bit ? d1r_ : d0r, bit ? d1i_ : d0i, v[j]);
+  }
+}
+
+// parity diagonal: factor d[bit(a) ^ bit(b)]
+template <typename R, int NR>
+__device__ __forceinline__ void diagp_any(typename Amp<R>::type (&v)[1 << NR], const R* m, int a,
+                                          int bq, uint32_t l0, const uint32_t (&off)[1 << NR],
+                                          uint32_t base) {
+  const uint32_t gpar = (a < 0 ? ((base >> (-a - 1)) & 1u) : 0u) ^
+                        (bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u);
+  const uint32_t pm = (a < 0 ? 0u : (1u << a)) | (bq < 0 ? 0u : (1u << bq));
+  const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const uint32_t bit = (__popc((l0 | off[j]) & pm) & 1u) ^ gpar;
+    v[j] = cmul(bit ? d1r_ : d0r, bit ? d1i_ : d0i, v[j]);
+  }
+}
+
+// general two-bit diagonal, factor d[2 bit(a) + bit(b)]
+template <typename R, int NR>
+__device__ __forceinline__ void diag2_any(typename Amp<R>::type (&v)[1 << NR], const R* m, int a,
+                                          int bq, uint32_t l0, const uint32_t (&off)[1 << NR],
+                                          uint32_t base) {
+  const uint32_t ga = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
+  const uint32_t gbb = bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u;
+  const int sa = a < 0 ? 0 : a, sb = bq < 0 ? 0 : bq;
+  const uint32_t ma = a < 0 ? 0u : 1u, mb = bq < 0 ? 0u : 1u;
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const uint32_t li = l0 | off[j];
+    const uint32_t k = ((((li >> sa) & ma) | ga) << 1) | (((li >> sb) & mb) | gbb);
+    v[j] = cmul(m[2 * k], m[2 * k + 1], v[j]);
+  }
+}
+
 template <int NR, typename F>
 __device__ __forceinline__ void dispatch1(int a, F&& f) {
   switch (a) {
@@ -651,51 +704,15 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
           SC_G1ALLQ_CASE(9) SC_G1ALLQ_CASE(10) SC_G1ALLQ_CASE(11) SC_G1ALLQ_CASE(12)
           SC_G1ALLQ_CASE(13) SC_G1ALLQ_CASE(14) SC_G1ALLQ_CASE(15)
 #undef SC_G1ALLQ_CASE
-          case SK_D1 << 4: {
-            // diag(d0, d1) on one bit; the bit is a tile position (a >= 0) or a
-            // global qubit fixed for the whole tile (a < 0)
-            const int a = g.a;
-            const uint32_t gb = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
-            const int sh = a < 0 ? 0 : a;
-            const uint32_t lm = a < 0 ? 0u : 1u;
-            const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
-#pragma unroll
-            for (int j = 0; j < NV; ++j) {
-              const uint32_t li = l0 | off[j];
-              if ((li & lmask) != lmask) continue;
-              const uint32_t bit = ((li >> sh) & lm) | gb;
-              v[j] = cmul(bit ? d1r_ : d0r, bit ? d1i_ : d0i, v[j]);
-            }
+          case SK_D1 << 4:
+            diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
             break;
-          }
-          case SK_DP << 4: {
-            // parity diagonal: factor d[bit(a) ^ bit(b)]
-            const int a = g.a, bq = g.b;
-            const uint32_t gpar = (a < 0 ? ((base >> (-a - 1)) & 1u) : 0u) ^
-                                  (bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u);
-            const uint32_t pm = (a < 0 ? 0u : (1u << a)) | (bq < 0 ? 0u : (1u << bq));
-            const R d0r = m[0], d0i = m[1], d1r_ = m[2], d1i_ = m[3];
-#pragma unroll
-            for (int j = 0; j < NV; ++j) {
-              const uint32_t bit = (__popc((l0 | off[j]) & pm) & 1u) ^ gpar;
-              v[j] = cmul(bit ? d1r_ : d0r, bit ? d1i_ : d0i, v[j]);
-            }
+          case SK_DP << 4:
+            diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
             break;
-          }
-          case SK_D2 << 4: {
-            const int a = g.a, bq = g.b;
-            const uint32_t ga = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
-            const uint32_t gbb = bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u;
-            const int sa = a < 0 ? 0 : a, sb = bq < 0 ? 0 : bq;
-            const uint32_t ma = a < 0 ? 0u : 1u, mb = bq < 0 ? 0u : 1u;
-#pragma unroll
-            for (int j = 0; j < NV; ++j) {
-              const uint32_t li = l0 | off[j];
-              const uint32_t k = ((((li >> sa) & ma) | ga) << 1) | (((li >> sb) & mb) | gbb);
-              v[j] = cmul(m[2 * k], m[2 * k + 1], v[j]);
-            }
+          case SK_D2 << 4:
+            diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
             break;
-          }
           default: break;
         }
       }
@@ -736,6 +753,208 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
     }
     if (producer) bulk_wait_all();
   }
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint reverse pass, fused (addition; the reference has no gradient API).
+// The plan holds the inverse gates in reverse order with a probe record before
+// each parametrised gate.  One launch carries both states (psi and lambda)
+// through the sweep tile by tile: every gate record is applied to both, and a
+// probe adds Im sum conj(lambda_i) (P psi)_i over the tile to its gradient slot
+// (P the gate's Pauli generator on a register bit).  Probe sums go warp ->
+// shared slot per warp -> per-CTA partial, and are added up in a fixed order.
+// ---------------------------------------------------------------------------
+
+// the record kinds of an adjoint plan (1-qubit matrix records, permutations,
+// diagonals; plans with dense 2-qubit records take the gate-by-gate path)
+template <typename R, int NR>
+__device__ __forceinline__ void apply_record(typename Amp<R>::type (&v)[1 << NR], const SwGate& g,
+                                             const R* m, uint32_t l0,
+                                             const uint32_t (&off)[1 << NR], uint32_t base) {
+  const uint32_t lmask = g.lmask;
+  switch (g.code) {
+#define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask)
+#define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask)
+#define SC_DO_D1R(A) d1r<R, NR, A>(v, m)
+#define SC_DO_CX(A, B) cxswap<R, NR, A, B>(v, l0, lmask)
+#define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m)
+#define SC_DO_SWAP(A, B) rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v)
+#define SC_DO_X0(A) xswap0<R, NR, A>(v)
+#define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v)
+    SC_CASES_1(SK_G1, SC_DO_G1)
+    SC_CASES_1(SK_X, SC_DO_X)
+    SC_CASES_1(SK_D1R, SC_DO_D1R)
+    SC_CASES_2(SK_CX, SC_DO_CX)
+    SC_CASES_2(SK_DPR, SC_DO_DPR)
+    SC_CASES_2(SK_SWAP, SC_DO_SWAP)
+    SC_CASES_1(SK_X0, SC_DO_X0)
+    SC_CASES_2(SK_CX0, SC_DO_CX0)
+#undef SC_DO_G1
+#undef SC_DO_X
+#undef SC_DO_D1R
+#undef SC_DO_CX
+#undef SC_DO_DPR
+#undef SC_DO_SWAP
+#undef SC_DO_X0
+#undef SC_DO_CX0
+#define SC_G1ALL_CASE(M)                        \
+  case (SK_G1ALL << 4) | (M):                   \
+    if constexpr (((M) >> NR) == 0) {           \
+      g1all<R, NR, (M)>(v, m, l0, off);         \
+    }                                           \
+    break;
+    SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
+    SC_G1ALL_CASE(5) SC_G1ALL_CASE(6) SC_G1ALL_CASE(7) SC_G1ALL_CASE(8)
+    SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
+    SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
+#undef SC_G1ALL_CASE
+    case SK_D1 << 4:
+      diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
+      break;
+    case SK_DP << 4:
+      diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+      break;
+    case SK_D2 << 4:
+      diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+      break;
+    default: break;
+  }
+}
+
+// Im sum_j conj(w_j) (P v)_j over the thread's registers, P the Pauli PAULI_
+// (1 = X, 2 = Y = iXZ, 3 = Z) on register bit A_ (the planner puts a probed
+// qubit in the registers)
+template <typename R, int NR, int A_, int PAULI_>
+__device__ __forceinline__ double probe_sum(const typename Amp<R>::type (&v)[1 << NR],
+                                            const typename Amp<R>::type (&w)[1 << NR]) {
+  double s = 0.0;
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const int src = PAULI_ == 3 ? j : j ^ (1 << A_);  // X and Y move the partner in
+    double pr = (double)v[src].x, pi = (double)v[src].y;
+    if (PAULI_ != 1 && ((src >> A_) & 1)) {  // the Z factor: sign of the source bit
+      pr = -pr;
+      pi = -pi;
+    }
+    if (PAULI_ == 2) {  // Y = i X Z
+      const double t = pr;
+      pr = -pi;
+      pi = t;
+    }
+    s += (double)w[j].x * pi - (double)w[j].y * pr;
+  }
+  return s;
+}
+
+template <typename R, int NR>
+__global__ void __launch_bounds__(256)
+    k_adjoint_sweep(typename Amp<R>::type* __restrict__ psi, typename Amp<R>::type* __restrict__ lam,
+                    const __grid_constant__ SweepParams<R> p, double* __restrict__ partial,
+                    int n_probes) {
+  using A = typename Amp<R>::type;
+  constexpr int NV = 1 << NR;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const uint32_t tile_amps = 1u << p.T;
+  A* const bp = reinterpret_cast<A*>(smem_raw);
+  A* const bl = bp + tile_amps;
+  double* const acc = reinterpret_cast<double*>(bl + tile_amps);  // [probe][warp]
+  const uint32_t tid = threadIdx.x;
+  const uint32_t nwarps = blockDim.x >> 5;  // blockDim.x is a multiple of 32 (host check)
+  const uint32_t warp = tid >> 5;
+  for (uint32_t k = tid; k < (uint32_t)n_probes * nwarps; k += blockDim.x) acc[k] = 0.0;
+  __syncthreads();
+  const int ns = p.n_stages;
+  const uint32_t l0_first = stage_l0<NR>(tid, p.stages[0]);
+  const uint32_t l0_last = stage_l0<NR>(tid, p.stages[ns - 1]);
+  const uint32_t gt_first = spread32(l0_first, p);
+  const uint32_t gt_last = spread_out32(l0_last, p);
+  for (uint32_t t = blockIdx.x; t < (uint32_t)p.tiles; t += gridDim.x) {
+    const uint32_t base = tile_base(t, p);
+    A v[NV], w[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      v[j] = psi[base | gt_first | p.gfirst[j]];
+      w[j] = lam[base | gt_first | p.gfirst[j]];
+    }
+    uint32_t l0 = l0_first, off[NV], sidx[NV];
+#pragma unroll 1
+    for (int s = 0; s < ns; ++s) {
+      const SwStage& stg = p.stages[s];
+      const SwStageTab& tab = p.tabs[s];
+      const uint32_t nl0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
+      const uint32_t sw0 = swz<R>(nl0);
+      if (s > 0) {
+        __syncthreads();  // readers of the buffers are done
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+          bp[sidx[j]] = v[j];
+          bl[sidx[j]] = w[j];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < NV; ++j) {
+          v[j] = bp[sw0 ^ tab.soff[j]];
+          w[j] = bl[sw0 ^ tab.soff[j]];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.wsoff[j];
+      l0 = nl0;
+#pragma unroll
+      for (int j = 0; j < NV; ++j) off[j] = tab.off[j];
+#pragma unroll 1
+      for (int gi = stg.g0; gi < stg.g1; ++gi) {
+        const SwGate& g = p.gates[gi];
+        if (((uint64_t)base & g.gmask) != g.gmask) continue;
+        if (g.kind == SK_PROBE) {
+          double ps = 0.0;
+          switch (g.code & 15) {
+#define SC_PROBE_CASE(A, P)                      \
+  case ((A) << 2) | (P):                         \
+    if constexpr ((A) < NR) ps = probe_sum<R, NR, (A), (P)>(v, w); \
+    break;
+            SC_PROBE_CASE(0, 1) SC_PROBE_CASE(0, 2) SC_PROBE_CASE(0, 3)
+            SC_PROBE_CASE(1, 1) SC_PROBE_CASE(1, 2) SC_PROBE_CASE(1, 3)
+            SC_PROBE_CASE(2, 1) SC_PROBE_CASE(2, 2) SC_PROBE_CASE(2, 3)
+            SC_PROBE_CASE(3, 1) SC_PROBE_CASE(3, 2) SC_PROBE_CASE(3, 3)
+#undef SC_PROBE_CASE
+            default: break;
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
+          if ((tid & 31u) == 0) acc[(uint32_t)g.b * nwarps + warp] += ps;  // b: local probe index
+          continue;
+        }
+        apply_record<R, NR>(v, g, p.pool + g.moff, l0, off, base);
+        apply_record<R, NR>(w, g, p.pool + g.moff, l0, off, base);
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      psi[base | gt_last | p.glast[j]] = v[j];
+      lam[base | gt_last | p.glast[j]] = w[j];
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = tid; k < (uint32_t)n_probes; k += blockDim.x) {
+    double sum = 0.0;
+    for (uint32_t q = 0; q < nwarps; ++q) sum += acc[k * nwarps + q];
+    partial[(size_t)blockIdx.x * (size_t)n_probes + k] = sum;
+  }
+}
+
+// grad[slot[k]] += sum over CTAs of partial[cta][k], CTAs in order (one thread per probe)
+struct ProbeSlots {
+  int32_t slot[kSweepMaxGates];
+};
+
+__global__ void k_probe_reduce(const double* __restrict__ partial, int ctas, int n_probes,
+                               const __grid_constant__ ProbeSlots slots, double* __restrict__ grad) {
+  const int k = (int)threadIdx.x;
+  if (k >= n_probes) return;
+  double sum = 0.0;
+  for (int b = 0; b < ctas; ++b) sum += partial[(size_t)b * (size_t)n_probes + k];
+  grad[slots.slot[k]] += sum;
 }
 
 struct LaunchCache {
@@ -935,6 +1154,75 @@ cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, co
   SweepParams<double> p;
   if (!fill(&p)) return cudaErrorInvalidValue;
   return launch_t<double>(states, p, err, sm_count, s);
+}
+
+bool adjoint_plan_supported(const Plan& plan) {
+  if (!plan.ok || !plan.restore.empty()) return false;
+  for (const SwSweep& sw : plan.sweeps) {
+    if (sw.nr != 3 || sw.T - sw.nr < 5 || sw.T - sw.nr > 8 || sw.relayout) return false;
+    if (!(sw.scale_re == 1.0 && sw.scale_im == 0.0)) return false;
+    for (int g = plan.stages[sw.s0].g0; g < plan.stages[sw.s1 - 1].g1; ++g) {
+      switch (plan.gates[g].kind) {
+        case SK_G1: case SK_X: case SK_SWAP: case SK_D1: case SK_D2: case SK_DP:
+        case SK_CX: case SK_DPR: case SK_G1ALL: case SK_D1R: case SK_X0: case SK_CX0:
+        case SK_PROBE:
+          break;
+        default: return false;
+      }
+    }
+  }
+  return true;
+}
+
+namespace {
+
+template <typename R>
+cudaError_t launch_adjoint_t(void* psi, void* lam, const Plan& plan, size_t k, double* partial,
+                             int max_ctas, double* grad, int sm_count, cudaStream_t s) {
+  using A = typename Amp<R>::type;
+  SweepParams<R> p;
+  if (!fill_params(plan, k, &p) || p.nr != 3) return cudaErrorInvalidValue;
+  // probe records carry the gradient slot; the kernel wants the local probe index
+  ProbeSlots slots;
+  int n_probes = 0;
+  const int ng = p.stages[p.n_stages - 1].g1;
+  for (int g = 0; g < ng; ++g) {
+    if (p.gates[g].kind != SK_PROBE) continue;
+    if (n_probes >= kSweepMaxGates) return cudaErrorInvalidValue;
+    slots.slot[n_probes] = p.gates[g].b;
+    p.gates[g].b = n_probes++;
+  }
+  const int threads = 1 << (p.T - p.nr);
+  if (threads < 32 || threads > 256) return cudaErrorInvalidValue;
+  const size_t smem = 2 * (sizeof(A) << p.T) + sizeof(double) * (size_t)n_probes * (threads / 32);
+  auto kern = k_adjoint_sweep<R, 3>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+  if (e != cudaSuccess) return e;
+  const int64_t grid =
+      std::max<int64_t>(1, std::min<int64_t>({p.tiles, (int64_t)sm_count * std::max(per_sm, 1),
+                                              (int64_t)max_ctas}));
+  kern<<<(unsigned)grid, threads, smem, s>>>(static_cast<A*>(psi), static_cast<A*>(lam), p,
+                                              partial, n_probes);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (n_probes > 0) {
+    k_probe_reduce<<<1, 128, 0, s>>>(partial, (int)grid, n_probes, slots, grad);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+}  // namespace
+
+cudaError_t launch_adjoint_sweep(int dtype, void* psi, void* lam, const Plan& plan, size_t k,
+                                 double* partial, int max_ctas, double* grad, int sm_count,
+                                 cudaStream_t s) {
+  if (dtype == SC_C64)
+    return launch_adjoint_t<float>(psi, lam, plan, k, partial, max_ctas, grad, sm_count, s);
+  return launch_adjoint_t<double>(psi, lam, plan, k, partial, max_ctas, grad, sm_count, s);
 }
 
 }  // namespace sc

@@ -23,6 +23,7 @@ double gate_cost(const PGate& g) {
     case PK_DIAG1:
     case PK_DIAG2: return 3.0;    // 1 complex multiply + bit tests
     case PK_PAULI: return 1.0;    // a register select / sign per trajectory
+    case PK_PROBE: return 2.0;    // one complex product per amplitude, reduced
     default: return 0.5;          // register selects
   }
 }
@@ -41,6 +42,7 @@ uint64_t dense_mask(const PGate& g) {
   switch (g.kind) {
     case PK_DENSE1:
     case PK_PAULI:
+    case PK_PROBE:
     case PK_X: return 1ULL << g.q0;
     case PK_DENSE2:
     case PK_SWAP: return (1ULL << g.q0) | (1ULL << g.q1);
@@ -1008,6 +1010,11 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             sg.a = reg_of_pos[pos_of[pg.q0]];
             sg.b = pg.q1;  // slot
             break;
+          case PK_PROBE:
+            sg.kind = SK_PROBE;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            sg.b = (int32_t)pg.op_index;  // gradient slot
+            break;
           case PK_DIAG1:
             sg.kind = SK_D1;
             sg.a = ref(pg.q0);
@@ -1037,7 +1044,8 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         }
         if (sg.kind == SK_X && sg.lmask == 0) sg.kind = SK_X0;
         if (sg.kind == SK_CX && sg.lmask == 0) sg.kind = SK_CX0;
-        sg.code = sw_code(sg.kind, sg.a, sg.b);
+        sg.code = sg.kind == SK_PROBE ? (SK_PROBE << 4) | (sg.a << 2) | (pg.q1 & 3)
+                                      : sw_code(sg.kind, sg.a, sg.b);
         plan.gates.push_back(sg);
         plan.gate_ops.push_back(pg.op_index);
       }

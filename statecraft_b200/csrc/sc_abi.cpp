@@ -471,6 +471,7 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
   if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) c->relayout = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_ROTATION")) c->rotation = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_PEEPHOLE")) c->peephole = atoi(v) != 0;
+  if (const char* v = getenv("STATECRAFT_B200_ADJOINT_FUSED")) c->adjoint_fused = atoi(v) != 0;
   *out_ctx = c;
   return SC_OK;
 }

@@ -1,12 +1,17 @@
 // Adjoint differentiation entry points (addition; the reference engine has no
 // gradient API).  Two device state buffers (psi, lambda), no stored intermediate
-// states: the reverse pass un-applies each gate from both.
+// states: the reverse pass un-applies each gate from both.  When the circuit fits
+// (1-qubit rotation generators, no dense 2-qubit gates) the reverse pass runs as
+// fused dual-state sweeps, each carrying both states through many inverse gates
+// and gradient probes; otherwise gate by gate, three passes per rotation.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
 
 #include "sc_adjoint.h"
 #include "sc_ctx.h"
+#include "sc_sweep.h"
 
 namespace sc {
 
@@ -44,6 +49,52 @@ bool generator(const sc_op& op, uint64_t* x, uint64_t* z) {
     case SC_OP_RZZ: *x = 0; *z = (1ULL << op.q0) | (1ULL << op.q1); return true;
     default: return false;
   }
+}
+
+// The inverse gates in reverse order, with a probe before each parametrised gate
+// (gradient slot = the op's parameter index).  False when some generator is not a
+// single-qubit Pauli (the gate-by-gate path handles those).
+bool reverse_gates(const Ctx* c, std::vector<PGate>& out) {
+  for (int64_t i = (int64_t)c->adj_ops.size() - 1; i >= 0; --i) {
+    const sc_op& op = c->adj_ops[i];
+    if (op.kind == SC_OP_MEASURE) continue;
+    PGate g;
+    bool produced = false;
+    normalise_op(op, c->adj_params.data(), (int64_t)c->adj_params.size(), &g, &produced);
+    if (!produced) continue;
+    uint64_t x = 0, z = 0;
+    if (op.param >= 0 && generator(op, &x, &z)) {
+      if (__builtin_popcountll(x | z) != 1) return false;
+      PGate pr;
+      std::memset(&pr, 0, sizeof pr);
+      pr.kind = PK_PROBE;
+      pr.q0 = __builtin_ctzll(x | z);
+      pr.q1 = x ? (z ? 2 : 1) : 3;  // X, Y = iXZ, Z
+      pr.op_index = op.param;
+      out.push_back(pr);
+    }
+    PGate inv = invert(g);
+    inv.op_index = i;
+    out.push_back(inv);
+  }
+  return true;
+}
+
+// Sweep shape of the reverse pass: 2048-amplitude tiles, 3 register qubits (both
+// states' registers in one thread), plain matrix records.
+PlanParams reverse_plan_params(const Ctx* c) {
+  PlanParams pp;
+  const bool c64 = c->cfg.dtype == SC_C64;
+  pp.tile_qubits = 11;
+  pp.low_qubits = c64 ? 5 : 4;
+  pp.nr = 3;
+  pp.budget = -1.0;
+  pp.max_gates = kSweepMaxGates;
+  pp.max_pool = kSweepMaxPool;
+  pp.relayout = false;
+  pp.rot_min_c = 0.0;
+  pp.peephole = false;
+  return pp;
 }
 
 }  // namespace
@@ -102,10 +153,15 @@ int32_t sc_adjoint_backward(void* p, double* out_grad, int64_t n_params) {
   const int blocks = adjoint_partial_blocks(n, c->sm_count);
   int rc = c->reserve(c->buf_adj_lambda, amp << n, "adjoint lambda");
   if (rc != SC_OK) return rc;
-  const size_t scratch = sizeof(double2) * (size_t)blocks + sizeof(double) * (size_t)(n_params + 1);
+  // partial sums: per block of the inner-product kernel (gate-by-gate path) or per
+  // CTA and probe of a fused reverse sweep
+  const int max_ctas = c->sm_count * 8;
+  const size_t partial_doubles =
+      std::max<size_t>(2 * (size_t)blocks, (size_t)max_ctas * (size_t)kSweepMaxGates);
+  const size_t scratch = sizeof(double) * (partial_doubles + (size_t)(n_params + 1));
   if ((rc = c->reserve(c->buf_adj_phi, scratch, "adjoint scratch")) != SC_OK) return rc;
   double2* partial = static_cast<double2*>(c->buf_adj_phi.p);
-  double* grad = reinterpret_cast<double*>(partial + blocks);
+  double* grad = static_cast<double*>(c->buf_adj_phi.p) + partial_doubles;
   cudaStream_t s = c->stream;
   void* psi = c->state.p;
   void* lam = c->buf_adj_lambda.p;
@@ -125,7 +181,25 @@ int32_t sc_adjoint_backward(void* p, double* out_grad, int64_t n_params) {
   c->mark_end();
   if (e != cudaSuccess) return fail_cuda(e, "adjoint H psi");
 
-  for (int64_t i = (int64_t)c->adj_ops.size() - 1; i >= 0; --i) {
+  bool fused = false;
+  if (c->adjoint_fused) {
+    std::vector<PGate> rev;
+    if (reverse_gates(c, rev)) {
+      const Plan plan = plan_sweeps(rev, n, reverse_plan_params(c));
+      if (adjoint_plan_supported(plan)) {
+        fused = true;
+        for (size_t k = 0; k < plan.sweeps.size() && e == cudaSuccess; ++k) {
+          c->mark_begin(KC_ADJOINT, 4.0 * dim * amp, 2);
+          e = launch_adjoint_sweep(c->cfg.dtype, psi, lam, plan, k,
+                                   static_cast<double*>(c->buf_adj_phi.p), max_ctas, grad,
+                                   c->sm_count, s);
+          c->mark_end();
+        }
+        if (e != cudaSuccess) return fail_cuda(e, "adjoint reverse sweep");
+      }
+    }
+  }
+  for (int64_t i = (int64_t)c->adj_ops.size() - 1; i >= 0 && !fused; --i) {
     const sc_op& op = c->adj_ops[i];
     if (op.kind == SC_OP_MEASURE) continue;
     PGate g;

@@ -40,6 +40,7 @@ struct Ctx {
   bool relayout = true;
   bool rotation = true;  // rotation form for 1-qubit unitaries in sweeps
   bool peephole = true;  // per-stage record peephole in the planner
+  bool adjoint_fused = true;  // adjoint reverse pass as dual-state sweeps when it fits
 
   // state
   int n = 0;

@@ -23,7 +23,11 @@ namespace sc {
 //   PK_DIAG2   diag(d[4]) on (q0 = first, q1 = second)          m[0..7]
 //   PK_PAULI   Pauli slot on q0 (batched trajectories): the Pauli (I, X, Y or Z)
 //              is chosen per trajectory; q1 = slot index into the choice table
-enum PKind : int32_t { PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2, PK_PAULI };
+// PK_PROBE (adjoint reverse pass only): q0 = qubit, q1 = Pauli generator (1 = X,
+// 2 = Y, 3 = Z), op_index = gradient slot; adds Im <lambda| P |psi> to that slot.
+enum PKind : int32_t {
+  PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2, PK_PAULI, PK_PROBE
+};
 
 struct PGate {
   int32_t kind;
@@ -74,9 +78,11 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        other controls lie outside the registers (lmask: tile positions, gmask:
 //        global qubits), last to touch its bits in a stage that is not the sweep's
 //        last: applied to the stage's exit slots instead of the registers.
+// SK_PROBE: gradient probe on register bit a, generator Pauli in the code's low two
+//        bits (1 = X, 2 = Y, 3 = Z), b = gradient slot (the adjoint reverse sweep).
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
@@ -221,6 +227,16 @@ cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int
 cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, const Plan& plan,
                                size_t k, const uint8_t* paulis, int n_slots, int* err,
                                int sm_count, cudaStream_t s);
+// Fused adjoint reverse pass (plans of inverse gates with SK_PROBE records):
+// adjoint_plan_supported says whether every sweep fits the dual-state kernel
+// (register qubits 3, at least 32 threads per tile, matrix / permutation /
+// diagonal records only, no rotation scalar, no layout change); the launcher runs
+// sweep k on psi and lambda and adds its probe sums to grad[slot] through
+// `partial` (room for max_ctas x kSweepMaxGates doubles).
+bool adjoint_plan_supported(const Plan& plan);
+cudaError_t launch_adjoint_sweep(int dtype, void* psi, void* lam, const Plan& plan, size_t k,
+                                 double* partial, int max_ctas, double* grad, int sm_count,
+                                 cudaStream_t s);
 // in-place qubit-bit permutation of an n-qubit state
 cudaError_t launch_permute(int dtype, void* state, int n, const SwPerm& perm, int sm_count,
                            cudaStream_t s);
