@@ -847,7 +847,7 @@ __device__ __forceinline__ double probe_sum(const typename Amp<R>::type (&v)[1 <
 }
 
 template <typename R, int NR>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
     k_adjoint_sweep(typename Amp<R>::type* __restrict__ psi, typename Amp<R>::type* __restrict__ lam,
                     const __grid_constant__ SweepParams<R> p, double* __restrict__ partial,
                     int n_probes) {
