@@ -52,9 +52,21 @@ bool generator(const sc_op& op, uint64_t* x, uint64_t* z) {
 }
 
 // The inverse gates in reverse order, with a probe before each parametrised gate
-// (gradient slot = the op's parameter index).  False when some generator is not a
-// single-qubit Pauli (the gate-by-gate path handles those).
+// (gradient slot = the op's parameter index).  Within a run of parametrised
+// rotations on distinct qubits all probes come first: a probe on qubit q commutes
+// with gates on other qubits (they act on both states), so the inverse rotations
+// of the run stay adjacent and group into one record per stage.  False when some
+// generator is not a single-qubit Pauli (the gate-by-gate path handles those).
 bool reverse_gates(const Ctx* c, std::vector<PGate>& out) {
+  std::vector<PGate> probes, gates;
+  uint64_t run_qubits = 0;
+  auto flush = [&]() {
+    out.insert(out.end(), probes.begin(), probes.end());
+    out.insert(out.end(), gates.begin(), gates.end());
+    probes.clear();
+    gates.clear();
+    run_qubits = 0;
+  };
   for (int64_t i = (int64_t)c->adj_ops.size() - 1; i >= 0; --i) {
     const sc_op& op = c->adj_ops[i];
     if (op.kind == SC_OP_MEASURE) continue;
@@ -62,21 +74,28 @@ bool reverse_gates(const Ctx* c, std::vector<PGate>& out) {
     bool produced = false;
     normalise_op(op, c->adj_params.data(), (int64_t)c->adj_params.size(), &g, &produced);
     if (!produced) continue;
+    PGate inv = invert(g);
+    inv.op_index = i;
     uint64_t x = 0, z = 0;
     if (op.param >= 0 && generator(op, &x, &z)) {
-      if (__builtin_popcountll(x | z) != 1) return false;
+      const uint64_t q = x | z;
+      if (__builtin_popcountll(q) != 1) return false;
+      if (run_qubits & q || (touch_mask(inv) & ~q)) flush();
       PGate pr;
       std::memset(&pr, 0, sizeof pr);
       pr.kind = PK_PROBE;
-      pr.q0 = __builtin_ctzll(x | z);
+      pr.q0 = __builtin_ctzll(q);
       pr.q1 = x ? (z ? 2 : 1) : 3;  // X, Y = iXZ, Z
       pr.op_index = op.param;
-      out.push_back(pr);
+      probes.push_back(pr);
+      gates.push_back(inv);
+      run_qubits |= q;
+      continue;
     }
-    PGate inv = invert(g);
-    inv.op_index = i;
+    flush();
     out.push_back(inv);
   }
+  flush();
   return true;
 }
 
