@@ -4,6 +4,8 @@
 //   lambda = H psi;  for gates k = N..1:  if G_k = exp(-i t/2 P):
 //       dE/dt += Im <lambda | P | psi>;   psi <- G_k^dag psi;  lambda <- G_k^dag lambda
 // Inner products and the Pauli-sum application accumulate in FP64.
+#include <algorithm>
+
 #include "sc_adjoint.h"
 #include "sc_device.cuh"
 #include "sc_internal.h"
@@ -24,31 +26,43 @@ __device__ __forceinline__ void times_i_pow(int ny, double& r, double& i) {
   }
 }
 
-// out (+)= c * P psi
+// out (+)= sum_k c_k P_k psi for up to kSumTerms terms in one pass: per amplitude the
+// terms are summed in FP64 in order and `out` is written once (for 32 consecutive i
+// the partners i ^ x_k stay within one aligned 32-block, so the reads coalesce)
+constexpr int kSumTerms = 64;
+
+struct PauliTerms {
+  uint64_t x[kSumTerms], z[kSumTerms];
+  double c[kSumTerms];
+  int32_t count, accumulate;
+};
+
 template <typename R>
-__global__ void k_pauli_accumulate(const typename Amp<R>::type* __restrict__ psi,
-                                   typename Amp<R>::type* __restrict__ out, int n, uint64_t x,
-                                   uint64_t z, double c, int accumulate) {
-  const int ny = __popcll(x & z) & 3;
+__global__ void k_pauli_sum(const typename Amp<R>::type* __restrict__ psi,
+                            typename Amp<R>::type* __restrict__ out, int n,
+                            const __grid_constant__ PauliTerms t) {
   const uint64_t dim = 1ULL << n;
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < dim;
        i += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t j = i ^ x;
-    const auto a = psi[j];
-    double r = a.x, im = a.y;
-    if (__popcll(z & j) & 1) {
-      r = -r;
-      im = -im;
-    }
-    times_i_pow(ny, r, im);
-    r *= c;
-    im *= c;
-    if (accumulate) {
+    double sr = 0.0, si = 0.0;
+    if (t.accumulate) {
       const auto o = out[i];
-      r += (double)o.x;
-      im += (double)o.y;
+      sr = (double)o.x;
+      si = (double)o.y;
     }
-    out[i] = make_amp<R>((R)r, (R)im);
+    for (int k = 0; k < t.count; ++k) {
+      const uint64_t j = i ^ t.x[k];
+      const auto a = psi[j];
+      double r = a.x, im = a.y;
+      if (__popcll(t.z[k] & j) & 1) {
+        r = -r;
+        im = -im;
+      }
+      times_i_pow(__popcll(t.x[k] & t.z[k]), r, im);
+      sr = fma(t.c[k], r, sr);
+      si = fma(t.c[k], im, si);
+    }
+    out[i] = make_amp<R>((R)sr, (R)si);
   }
 }
 
@@ -117,19 +131,29 @@ int blocks_for(int n, int sm_count) {
 
 int adjoint_partial_blocks(int n, int sm_count) { return blocks_for(n, sm_count); }
 
-cudaError_t launch_pauli_accumulate(int dtype, const void* psi, void* out, int n, uint64_t x,
-                                    uint64_t z, double c, bool accumulate, int sm_count,
-                                    cudaStream_t s) {
+cudaError_t launch_pauli_sum(int dtype, const void* psi, void* out, int n, const uint64_t* x,
+                             const uint64_t* z, const double* c, int64_t count, int sm_count,
+                             cudaStream_t s) {
   const int grid = blocks_for(n, sm_count);
-  if (dtype == SC_C64)
-    k_pauli_accumulate<float><<<grid, kThreads, 0, s>>>(static_cast<const float2*>(psi),
-                                                        static_cast<float2*>(out), n, x, z, c,
-                                                        accumulate ? 1 : 0);
-  else
-    k_pauli_accumulate<double><<<grid, kThreads, 0, s>>>(static_cast<const double2*>(psi),
-                                                         static_cast<double2*>(out), n, x, z, c,
-                                                         accumulate ? 1 : 0);
-  return cudaGetLastError();
+  for (int64_t k0 = 0; k0 < count; k0 += kSumTerms) {
+    PauliTerms t;
+    t.count = (int32_t)std::min<int64_t>(kSumTerms, count - k0);
+    t.accumulate = k0 > 0;
+    for (int k = 0; k < t.count; ++k) {
+      t.x[k] = x[k0 + k];
+      t.z[k] = z[k0 + k];
+      t.c[k] = c[k0 + k];
+    }
+    if (dtype == SC_C64)
+      k_pauli_sum<float><<<grid, kThreads, 0, s>>>(static_cast<const float2*>(psi),
+                                                   static_cast<float2*>(out), n, t);
+    else
+      k_pauli_sum<double><<<grid, kThreads, 0, s>>>(static_cast<const double2*>(psi),
+                                                    static_cast<double2*>(out), n, t);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t launch_generator_grad(int dtype, const void* lam, const void* psi, int n, uint64_t x,

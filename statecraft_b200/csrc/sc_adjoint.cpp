@@ -189,13 +189,14 @@ int32_t sc_adjoint_backward(void* p, double* out_grad, int64_t n_params) {
   if (e != cudaSuccess) return fail_cuda(e, "gradient init");
 
   // lambda = H psi
-  c->mark_begin(KC_ADJOINT, 3.0 * dim * amp * (double)c->adj_c.size(), (int)c->adj_c.size());
+  // one read of psi per term, one write of lambda per pass of up to 64 terms
+  const int sum_passes = (int)((c->adj_c.size() + 63) / 64);
+  c->mark_begin(KC_ADJOINT, dim * amp * (double)(c->adj_c.size() + sum_passes), sum_passes);
   if (c->adj_c.empty()) {
     e = cudaMemsetAsync(lam, 0, amp << n, s);
   } else {
-    for (size_t t = 0; t < c->adj_c.size() && e == cudaSuccess; ++t)
-      e = launch_pauli_accumulate(c->cfg.dtype, psi, lam, n, c->adj_x[t], c->adj_z[t], c->adj_c[t],
-                                  t > 0, c->sm_count, s);
+    e = launch_pauli_sum(c->cfg.dtype, psi, lam, n, c->adj_x.data(), c->adj_z.data(),
+                         c->adj_c.data(), (int64_t)c->adj_c.size(), c->sm_count, s);
   }
   c->mark_end();
   if (e != cudaSuccess) return fail_cuda(e, "adjoint H psi");

@@ -8,11 +8,10 @@ namespace sc {
 
 int adjoint_partial_blocks(int n, int sm_count);
 
-// out = c * P psi (accumulate = false) or out += c * P psi
-cudaError_t launch_pauli_accumulate(int dtype, const void* psi, void* out, int n, uint64_t x,
-                                    uint64_t z, double c, bool accumulate, int sm_count,
-                                    cudaStream_t s);
-
+// out = sum_k c_k P_k psi (terms applied up to 64 per pass, FP64 sums)
+cudaError_t launch_pauli_sum(int dtype, const void* psi, void* out, int n, const uint64_t* x,
+                             const uint64_t* z, const double* c, int64_t count, int sm_count,
+                             cudaStream_t s);
 // grad[slot] += Im <lam | P | psi>, P = i^{|x&z|} X^x Z^z
 cudaError_t launch_generator_grad(int dtype, const void* lam, const void* psi, int n, uint64_t x,
                                   uint64_t z, double2* partial, double* grad, int slot,
