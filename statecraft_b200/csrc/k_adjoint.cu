@@ -156,6 +156,20 @@ cudaError_t launch_pauli_sum(int dtype, const void* psi, void* out, int n, const
   return cudaSuccess;
 }
 
+cudaError_t launch_inner(int dtype, const void* lam, const void* psi, int n, double2* partial,
+                         int sm_count, cudaStream_t s) {
+  const int grid = blocks_for(n, sm_count);
+  if (dtype == SC_C64)
+    k_pauli_inner<float><<<grid, kThreads, 0, s>>>(static_cast<const float2*>(lam),
+                                                   static_cast<const float2*>(psi), n, 0, 0,
+                                                   partial);
+  else
+    k_pauli_inner<double><<<grid, kThreads, 0, s>>>(static_cast<const double2*>(lam),
+                                                    static_cast<const double2*>(psi), n, 0, 0,
+                                                    partial);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_generator_grad(int dtype, const void* lam, const void* psi, int n, uint64_t x,
                                   uint64_t z, double2* partial, double* grad, int slot,
                                   int sm_count, cudaStream_t s) {

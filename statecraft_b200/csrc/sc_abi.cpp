@@ -309,6 +309,7 @@ int Ctx::ensure_state(int nq) {
 int Ctx::run(int nq, const sc_op* ops, int64_t n_ops, const double* init, uint64_t basis,
              bool has_basis, const double* params, int64_t n_params) {
   state_valid = false;
+  adj_ready = false;  // a pending adjoint pair refers to the state this run replaces
   // a noise schedule applies to one run only
   std::vector<sc_channel> noise_sched;
   noise_sched.swap(this->noise);

@@ -99,6 +99,19 @@ bool reverse_gates(const Ctx* c, std::vector<PGate>& out) {
   return true;
 }
 
+// doubles of partial sums in buf_adj_phi ahead of the gradient: per block of the
+// inner-product kernels (gate-by-gate path, <H>) or per CTA and probe of a fused
+// reverse sweep
+size_t partial_doubles(const Ctx* c) {
+  const int blocks = adjoint_partial_blocks(c->n, c->sm_count);
+  return std::max<size_t>(2 * (size_t)blocks, (size_t)c->sm_count * 8 * (size_t)kSweepMaxGates);
+}
+
+int reserve_scratch(Ctx* c, int64_t n_params) {
+  return c->reserve(c->buf_adj_phi, sizeof(double) * (partial_doubles(c) + (size_t)(n_params + 1)),
+                    "adjoint scratch");
+}
+
 // Sweep shape of the reverse pass: 2048-amplitude tiles, 3 register qubits (both
 // states' registers in one thread), plain matrix records.
 PlanParams reverse_plan_params(const Ctx* c) {
@@ -145,10 +158,39 @@ int32_t sc_adjoint_forward(void* p, int32_t n_qubits, const sc_op* ops, int64_t 
   }
   int rc = c->run(n_qubits, ops, n_ops, nullptr, 0, false, params, n_params);
   if (rc != SC_OK) return rc;
-  std::vector<double> terms;
-  if ((rc = c->pauli_terms(n_terms, xmask, zmask, terms)) != SC_OK) return rc;
+  const int n = c->n;
+  const uint64_t full = (n >= 64) ? ~0ULL : ((1ULL << n) - 1ULL);
+  for (int32_t t = 0; t < n_terms; ++t)
+    if ((xmask[t] | zmask[t]) & ~full)
+      return fail(SC_EINVAL, "Pauli term %d acts outside the register", t);
+  // lambda = H psi (the backward pass starts from it); <H> = Re <lambda | psi>
+  const size_t amp = (c->cfg.dtype == SC_C64) ? 8 : 16;
+  if ((rc = c->reserve(c->buf_adj_lambda, amp << n, "adjoint lambda")) != SC_OK) return rc;
+  if ((rc = reserve_scratch(c, n_params)) != SC_OK) return rc;
   double e = 0.0;
-  for (int32_t t = 0; t < n_terms; ++t) e += coeffs[t] * terms[t];
+  cudaStream_t s = c->stream;
+  const double dim = std::ldexp(1.0, n);
+  const int sum_passes = (n_terms + 63) / 64;
+  c->mark_begin(KC_ADJOINT, dim * amp * (double)(n_terms + sum_passes + 2), sum_passes + 1);
+  cudaError_t ce = cudaSuccess;
+  if (n_terms == 0) {
+    ce = cudaMemsetAsync(c->buf_adj_lambda.p, 0, amp << n, s);
+  } else {
+    const int blocks = adjoint_partial_blocks(n, c->sm_count);
+    ce = launch_pauli_sum(c->cfg.dtype, c->state.p, c->buf_adj_lambda.p, n, xmask, zmask, coeffs,
+                          n_terms, c->sm_count, s);
+    if (ce == cudaSuccess)
+      ce = launch_inner(c->cfg.dtype, c->buf_adj_lambda.p, c->state.p, n,
+                        static_cast<double2*>(c->buf_adj_phi.p), c->sm_count, s);
+    std::vector<double2> part(blocks);
+    if (ce == cudaSuccess)
+      ce = cudaMemcpyAsync(part.data(), c->buf_adj_phi.p, sizeof(double2) * (size_t)blocks,
+                           cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    for (int b = 0; b < blocks && ce == cudaSuccess; ++b) e += part[b].x;
+  }
+  c->mark_end();
+  if (ce != cudaSuccess) return fail_cuda(ce, "adjoint H psi");
   if (out_value) *out_value = e;
   c->adj_ops.assign(ops, ops + n_ops);
   c->adj_params.assign(params, params + n_params);
@@ -170,17 +212,11 @@ int32_t sc_adjoint_backward(void* p, double* out_grad, int64_t n_params) {
   const int n = c->n;
   const size_t amp = (c->cfg.dtype == SC_C64) ? 8 : 16;
   const int blocks = adjoint_partial_blocks(n, c->sm_count);
-  int rc = c->reserve(c->buf_adj_lambda, amp << n, "adjoint lambda");
+  int rc = reserve_scratch(c, n_params);  // lambda and the scratch came with the forward pass
   if (rc != SC_OK) return rc;
-  // partial sums: per block of the inner-product kernel (gate-by-gate path) or per
-  // CTA and probe of a fused reverse sweep
   const int max_ctas = c->sm_count * 8;
-  const size_t partial_doubles =
-      std::max<size_t>(2 * (size_t)blocks, (size_t)max_ctas * (size_t)kSweepMaxGates);
-  const size_t scratch = sizeof(double) * (partial_doubles + (size_t)(n_params + 1));
-  if ((rc = c->reserve(c->buf_adj_phi, scratch, "adjoint scratch")) != SC_OK) return rc;
   double2* partial = static_cast<double2*>(c->buf_adj_phi.p);
-  double* grad = static_cast<double*>(c->buf_adj_phi.p) + partial_doubles;
+  double* grad = static_cast<double*>(c->buf_adj_phi.p) + partial_doubles(c);
   cudaStream_t s = c->stream;
   void* psi = c->state.p;
   void* lam = c->buf_adj_lambda.p;
@@ -188,19 +224,7 @@ int32_t sc_adjoint_backward(void* p, double* out_grad, int64_t n_params) {
   cudaError_t e = cudaMemsetAsync(grad, 0, sizeof(double) * (size_t)(n_params + 1), s);
   if (e != cudaSuccess) return fail_cuda(e, "gradient init");
 
-  // lambda = H psi
-  // one read of psi per term, one write of lambda per pass of up to 64 terms
-  const int sum_passes = (int)((c->adj_c.size() + 63) / 64);
-  c->mark_begin(KC_ADJOINT, dim * amp * (double)(c->adj_c.size() + sum_passes), sum_passes);
-  if (c->adj_c.empty()) {
-    e = cudaMemsetAsync(lam, 0, amp << n, s);
-  } else {
-    e = launch_pauli_sum(c->cfg.dtype, psi, lam, n, c->adj_x.data(), c->adj_z.data(),
-                         c->adj_c.data(), (int64_t)c->adj_c.size(), c->sm_count, s);
-  }
-  c->mark_end();
-  if (e != cudaSuccess) return fail_cuda(e, "adjoint H psi");
-
+  // lambda = H psi was computed by the forward pass
   bool fused = false;
   if (c->adjoint_fused) {
     std::vector<PGate> rev;

@@ -57,3 +57,22 @@ def test_fused_complex64(monkeypatch):
     _, g64, _ = grad(18, 2, 55, dtype=A.SC_C64, fused=True, monkeypatch=monkeypatch)
     _, g128, _ = grad(18, 2, 55, fused=True, monkeypatch=monkeypatch)
     assert np.max(np.abs(g64 - g128)) < 1e-4
+
+
+def test_backward_after_another_run_is_rejected():
+    # the backward pass starts from the forward pass's state and lambda: a run on the
+    # same context in between replaces the state, so backward must refuse
+    from statecraft_b200.engine import serialize_circuit
+
+    ops, n_ops, n_params = W.hea_ops(10, 1)
+    params = W.hea_params(n_params, 3)
+    x, z, c = W.random_pauli_sum(10, 4, 4)
+    eng = AdjointEngine()
+    try:
+        eng.forward(10, ops, n_ops, params, x, z, c)
+        other, n_other = serialize_circuit(W.brickwall_circuit(10, 1, seed=5))
+        eng.ctx.run_ops(10, other, n_other)
+        with pytest.raises(A.IllegalStateException, match="preceding sc_adjoint_forward"):
+            eng.backward()
+    finally:
+        eng.close()
