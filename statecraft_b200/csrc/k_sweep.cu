@@ -765,22 +765,26 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 // shared slot per warp -> per-CTA partial, and are added up in a fixed order.
 // ---------------------------------------------------------------------------
 
-// the record kinds of an adjoint plan (1-qubit matrix records, permutations,
-// diagonals; plans with dense 2-qubit records take the gate-by-gate path)
+// A record of an adjoint plan (1-qubit matrix records, permutations, diagonals;
+// plans with dense 2-qubit records take the gate-by-gate path) applied to both
+// states in one dispatch: one join of the register state per record, not two.
 template <typename R, int NR>
-__device__ __forceinline__ void apply_record(typename Amp<R>::type (&v)[1 << NR], const SwGate& g,
-                                             const R* m, uint32_t l0,
-                                             const uint32_t (&off)[1 << NR], uint32_t base) {
+__device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 << NR],
+                                                  typename Amp<R>::type (&w)[1 << NR],
+                                                  const SwGate& g, const R* m, uint32_t l0,
+                                                  const uint32_t (&off)[1 << NR], uint32_t base) {
   const uint32_t lmask = g.lmask;
   switch (g.code) {
-#define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask)
-#define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask)
-#define SC_DO_D1R(A) d1r<R, NR, A>(v, m)
-#define SC_DO_CX(A, B) cxswap<R, NR, A, B>(v, l0, lmask)
-#define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m)
-#define SC_DO_SWAP(A, B) rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v)
-#define SC_DO_X0(A) xswap0<R, NR, A>(v)
-#define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v)
+#define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask), g1<R, NR, A>(w, m, l0, off, lmask)
+#define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask), xswap<R, NR, A>(w, l0, off, lmask)
+#define SC_DO_D1R(A) d1r<R, NR, A>(v, m), d1r<R, NR, A>(w, m)
+#define SC_DO_CX(A, B) cxswap<R, NR, A, B>(v, l0, lmask), cxswap<R, NR, A, B>(w, l0, lmask)
+#define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m), dpr<R, NR, A, B>(w, m)
+#define SC_DO_SWAP(A, B)                                          \
+  rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v), \
+      rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(w)
+#define SC_DO_X0(A) xswap0<R, NR, A>(v), xswap0<R, NR, A>(w)
+#define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v), cxswap0<R, NR, A, B>(w)
     SC_CASES_1(SK_G1, SC_DO_G1)
     SC_CASES_1(SK_X, SC_DO_X)
     SC_CASES_1(SK_D1R, SC_DO_D1R)
@@ -801,6 +805,7 @@ __device__ __forceinline__ void apply_record(typename Amp<R>::type (&v)[1 << NR]
   case (SK_G1ALL << 4) | (M):                   \
     if constexpr (((M) >> NR) == 0) {           \
       g1all<R, NR, (M)>(v, m, l0, off);         \
+      g1all<R, NR, (M)>(w, m, l0, off);         \
     }                                           \
     break;
     SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
@@ -810,12 +815,15 @@ __device__ __forceinline__ void apply_record(typename Amp<R>::type (&v)[1 << NR]
 #undef SC_G1ALL_CASE
     case SK_D1 << 4:
       diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
+      diag1_any<R, NR>(w, m, g.a, l0, off, lmask, base);
       break;
     case SK_DP << 4:
       diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+      diagp_any<R, NR>(w, m, g.a, g.b, l0, off, base);
       break;
     case SK_D2 << 4:
       diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+      diag2_any<R, NR>(w, m, g.a, g.b, l0, off, base);
       break;
     default: break;
   }
@@ -925,8 +933,7 @@ __global__ void __launch_bounds__(256, 2)
           if ((tid & 31u) == 0) acc[(uint32_t)g.b * nwarps + warp] += ps;  // b: local probe index
           continue;
         }
-        apply_record<R, NR>(v, g, p.pool + g.moff, l0, off, base);
-        apply_record<R, NR>(w, g, p.pool + g.moff, l0, off, base);
+        apply_record_pair<R, NR>(v, w, g, p.pool + g.moff, l0, off, base);
       }
     }
 #pragma unroll
