@@ -401,3 +401,29 @@ def test_memory_limit_reports_enomem():
         e.simulate(SimulationRequest.zeroState(Q.QuantumCircuit(20)))
     assert info.value.status == A.SC_ENOMEM
     e.close()
+
+
+@pytest.mark.parametrize("dtype,tol", [(A.SC_C128, 1e-12), (A.SC_C64, 2e-6)])
+def test_32_qubit_maximum_size(dtype, tol):
+    # the largest register the engine takes (2^32 amplitudes: 64 GiB c128, 32 GiB c64),
+    # where every tile and amplitude index uses the full 32 bits: GHZ-32, X on qubit
+    # 0, RY(1) on qubit 31; marginals and seeded samples against the closed form
+    n = 32
+    c = Q.QuantumCircuit(n).append(Q.Hadamard(), 0)
+    for q in range(n - 1):
+        c = c.append(Q.CnotGate.of(), q, q + 1)
+    c = c.append(Q.PauliX(), 0).append(Q.ry(1.0), n - 1)
+    ops, n_ops = serialize_circuit(c)
+    ctx = NativeContext(B200Config(dtype=dtype))
+    try:
+        ctx.run_ops(n, ops, n_ops)
+        cs, sn = math.cos(0.5) ** 2 / 2, math.sin(0.5) ** 2 / 2
+        np.testing.assert_allclose(ctx.probabilities([0, n - 1]), [sn, cs, cs, sn], rtol=0, atol=tol)
+        want = np.zeros(8)
+        want[0], want[7] = 0.5, 0.5  # qubits 5, 17, 26 follow the GHZ branches
+        np.testing.assert_allclose(ctx.probabilities([5, 17, 26]), want, rtol=0, atol=tol)
+        shots = ctx.sample([0, n - 1], 8192, 2024)
+        counts = np.bincount(shots, minlength=4)
+        assert np.all(np.abs(counts - 8192 * np.array([sn, cs, cs, sn])) < 6 * np.sqrt(8192 * 0.25))
+    finally:
+        ctx.close()
