@@ -203,6 +203,17 @@ __global__ void __launch_bounds__(1 << (kQT - NR), MB)
         const A* src = st + in.amp_off + (toff | tmap(n, ebase[kTop]));
 #pragma unroll
         for (int j = 0; j < NV; ++j) v[j] = src[tmap(n, (uint32_t)j << (kTop * NR))];
+        // the next item's amplitudes into L2 while this one computes (no registers,
+        // nothing to wait for): its loads then hit L2 instead of HBM
+        const int64_t wn = w + gridDim.x;
+        if (wn < a.n_items) {
+          QaoaInst inn;
+          uint32_t tn;
+          locate(wn, inn, tn);
+          const A* nsrc = st + inn.amp_off + (tile_off(inn.n, tn) | tmap(inn.n, ebase[kTop]));
+#pragma unroll
+          for (int j = 0; j < NV; ++j) prefetch_l2(nsrc + tmap(inn.n, (uint32_t)j << (kTop * NR)));
+        }
       }
     }
     auto has = [&](int G) { return ((smask >> (G * NR)) & (uint32_t)(NV - 1)) != 0u; };
