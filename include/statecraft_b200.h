@@ -248,6 +248,13 @@ SC_API int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, i
  * kernel's tile / stage / register semantics; returns the number of sweeps. */
 SC_API int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
                                 int32_t low_qubits, int32_t nr, double budget, double* state);
+/* As sc_debug_emulate_sweeps for one trajectory of a batch: Pauli slot j sits after
+ * op slot_after[j] (non-decreasing) on qubit slot_qubit[j] and applies paulis[j]
+ * (0 = I, 1 = X, 2 = Y, 3 = Z), planned the way sc_trajectories plans slots. */
+SC_API int32_t sc_debug_emulate_slots(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                               int32_t low_qubits, int32_t nr, double budget,
+                               const int64_t* slot_after, const int32_t* slot_qubit,
+                               int64_t n_slots, const uint8_t* paulis, double* state);
 
 #ifdef __cplusplus
 }

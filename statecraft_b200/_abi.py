@@ -148,6 +148,11 @@ SIGNATURES = {
     "sc_debug_emulate_sweeps": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                                  ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                  ctypes.c_double, _P(ctypes.c_double)]),
+    "sc_debug_emulate_slots": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
+                                                ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                ctypes.c_double, _P(ctypes.c_int64),
+                                                _P(ctypes.c_int32), ctypes.c_int64,
+                                                _P(ctypes.c_uint8), _P(ctypes.c_double)]),
 }
 
 PACKAGE_DIR = Path(__file__).resolve().parent

@@ -380,6 +380,34 @@ __device__ __forceinline__ void pauli(typename Amp<R>::type (&v)[1 << NR], uint3
   }
 }
 
+// Pauli slot conjugated through folded register permutations: i^p X^u Z^w over the
+// register bits, f = (u, w, p) of the trajectory's choice
+template <typename R, int NR>
+__device__ __forceinline__ void pauli_frame(typename Amp<R>::type (&v)[1 << NR], const R* f) {
+  const uint32_t u = (uint32_t)f[0], w = (uint32_t)f[1], ph = (uint32_t)f[2];
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j)
+    if (__popc(w & (uint32_t)j) & 1) v[j] = make_amp<R>(-v[j].x, -v[j].y);
+  if (u & 1u) xswap0<R, NR, 0>(v);
+  if constexpr (NR > 1) {
+    if (u & 2u) xswap0<R, NR, 1>(v);
+  }
+  if constexpr (NR > 2) {
+    if (u & 4u) xswap0<R, NR, 2>(v);
+  }
+  if constexpr (NR > 3) {
+    if (u & 8u) xswap0<R, NR, 3>(v);
+  }
+  if (ph & 1u) {
+#pragma unroll
+    for (int j = 0; j < (1 << NR); ++j) v[j] = make_amp<R>(-v[j].y, v[j].x);
+  }
+  if (ph & 2u) {
+#pragma unroll
+    for (int j = 0; j < (1 << NR); ++j) v[j] = make_amp<R>(-v[j].x, -v[j].y);
+  }
+}
+
 // switch cases for the dispatch code (sw_code): one jump per gate into code that
 // is specialised on its register bits
 #define SC_CASE_1(K, A, F) \
@@ -634,7 +662,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
         if (((uint64_t)base & g.gmask) != g.gmask) continue;
         if constexpr (kBatch) {
           // identity Pauli (the common branch): skip the record before the jump
-          if (g.kind == SK_PAULI && codes[g.b] == 0) continue;
+          if ((g.kind == SK_PAULI || g.kind == SK_PAULIF) && codes[g.b] == 0) continue;
         }
         const R* m = p.pool + g.moff;
         const uint32_t lmask = g.lmask;
@@ -663,6 +691,11 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #undef SC_DO_XF
 #undef SC_DO_CXF
           SC_CASES_1(SK_PAULI, SC_DO_PAULI)
+          case SK_PAULIF << 4:
+            if constexpr (kBatch) {
+              pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
+            }
+            break;
 #undef SC_DO_X0
 #undef SC_DO_CX0
 #undef SC_DO_PAULI
@@ -1113,7 +1146,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
     SwGate sg = plan.gates[g];
     if (sg.moff < pool_lo || sg.moff > pool_hi) return false;
     sg.moff -= pool_lo;
-    if (sg.kind == SK_PAULI) {  // slot -> local index into the staged choices
+    if (sg.kind == SK_PAULI || sg.kind == SK_PAULIF) {  // slot -> local index into the staged choices
       if (p->n_local_slots >= kSweepMaxGates) return false;
       p->slot_map[p->n_local_slots] = sg.b;
       sg.b = p->n_local_slots++;

@@ -34,6 +34,7 @@ int gate_pool_size(const PGate& g) {
     case PK_DENSE2: return 32;
     case PK_DIAG1: return 4;
     case PK_DIAG2: return 8;
+    case PK_PAULI: return 9;    // conjugated through folded permutations: (u, w, p) x 3
     default: return 0;
   }
 }
@@ -440,21 +441,60 @@ void optimize_stage(Plan& plan, int32_t g0, SwStage& st, const int* reg_of_pos,
       --i;
     }
   }
-  uint32_t later = folded_bits;
+  // Folds, decided backwards.  A plain permutation folds when no later record other
+  // than a Pauli slot touches its bits: the slots after it are conjugated below, and
+  // folded permutations may overlap (they compose in time order).  Slot folds of
+  // conditional permutations need every later record, slots included, off their bits.
+  const int ng = (int)G.size() - g0;
+  std::vector<char> fold(ng, 0);
+  uint32_t later_all = folded_bits, later = folded_bits;
   for (int k = (int)G.size() - 1; k >= g0; --k) {
     SwGate& g = G[k];
     const uint32_t f = record_bits(g, reg_of_pos);
-    if (!(f & later)) {
-      if (plain_permutation(g)) {
-        compose_permutation(st, g);
-        G.erase(G.begin() + k);
-      } else if (!last && conditional_permutation(g, reg_of_pos)) {
-        g.kind = (g.kind == SK_X0 || g.kind == SK_X) ? SK_XF : SK_CXF;
-        g.code = sw_code(g.kind, g.a, g.b);
-      }
+    if (plain_permutation(g) && !(f & later)) {
+      fold[k - g0] = 1;
+      later_all |= f;
+      continue;
     }
-    later |= f;
+    if (!last && !(f & later_all) && conditional_permutation(g, reg_of_pos)) {
+      g.kind = (g.kind == SK_X0 || g.kind == SK_X) ? SK_XF : SK_CXF;
+      g.code = sw_code(g.kind, g.a, g.b);
+    }
+    later_all |= f;
+    if (g.kind != SK_PAULI) later |= f;
   }
+  // Forwards: the folded permutations join the exit permutation in time order; a
+  // slot after some of them becomes P^dag S P, P their composition (x -> M x ^ c):
+  // X_a -> X^{M^-1 e_a}, Z_a -> (-1)^{c_a} Z^{M^T e_a}, Y_a = i X_a Z_a likewise.
+  SwStage pst;
+  for (int j = 0; j < 16; ++j) pst.perm[j] = (int8_t)j;
+  bool moved = false;
+  for (int k = g0; k < (int)G.size(); ++k) {
+    SwGate& g = G[k];
+    if (fold[k - g0]) {
+      compose_permutation(st, g);
+      compose_permutation(pst, g);
+      moved = true;
+      continue;
+    }
+    if (g.kind != SK_PAULI || !moved) continue;
+    const int a = g.a, c = pst.perm[0];
+    int u = 0, w = 0;
+    for (int x = 0; x < 16; ++x)
+      if ((pst.perm[x] ^ c) == (1 << a)) u = x;  // M^-1 e_a
+    for (int b = 0; b < 4; ++b) w |= (((pst.perm[1 << b] ^ c) >> a) & 1) << b;  // M^T e_a
+    const int sa = (c >> a) & 1;
+    if (u == (1 << a) && w == (1 << a) && sa == 0) continue;  // P commutes with the slot
+    g.kind = SK_PAULIF;
+    g.moff = (int32_t)plan.pool.size();
+    g.code = SK_PAULIF << 4;
+    const double frame[9] = {(double)u, 0.0, 0.0,                      // X
+                             (double)u, (double)w, (double)(1 + 2 * sa),  // Y = i X Z
+                             0.0, (double)w, (double)(2 * sa)};        // Z
+    plan.pool.insert(plan.pool.end(), frame, frame + 9);
+  }
+  for (int k = (int)G.size() - 1; k >= g0; --k)
+    if (fold[k - g0]) G.erase(G.begin() + k);
 }
 
 }  // namespace

@@ -80,7 +80,9 @@ inline C mac2(const double* m0, C a0, const double* m1, C a1) {
 // by tile position, the stages run on it (register j of a thread leaves the stage
 // at position l0 | off[perm[j]]), and the tile is scattered through the output
 // layout -- the kernel's shared-memory tile, exchanges and final store.
-void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
+// codes: the Pauli (0 = I, 1 = X, 2 = Y, 3 = Z) of each slot, for plans with slots
+void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
+                   const uint8_t* codes = nullptr) {
   // the kernel sees only the sweep's pool range: a record outside it poisons the state
   for (int gi = plan.stages[sw.s0].g0; gi < plan.stages[sw.s1 - 1].g1; ++gi)
     if (plan.gates[gi].moff < sw.pool0 || plan.gates[gi].moff > sw.pool1) {
@@ -137,6 +139,29 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw) {
               for (int j = 0; j < NV; ++j)
                 if (!(j & (1 << g.a))) std::swap(v[j], v[j | (1 << g.a)]);
               break;
+            case SK_PAULI:
+            case SK_PAULIF: {  // i^p X^u Z^w over the register bits
+              const int code = codes ? codes[g.b] : 0;
+              if (code == 0) break;
+              int u, w, ph;
+              if (g.kind == SK_PAULI) {
+                u = code != 3 ? 1 << g.a : 0;
+                w = code != 1 ? 1 << g.a : 0;
+                ph = code == 2 ? 1 : 0;
+              } else {
+                u = (int)m[3 * (code - 1)];
+                w = (int)m[3 * (code - 1) + 1];
+                ph = (int)m[3 * (code - 1) + 2];
+              }
+              const std::vector<C> src(v);
+              for (int j = 0; j < NV; ++j) {
+                C x = src[j ^ u];
+                if (__builtin_popcount(w & (j ^ u)) & 1) x = {-x.r, -x.i};
+                for (int q = 0; q < (ph & 3); ++q) x = {-x.i, x.r};
+                v[j] = x;
+              }
+              break;
+            }
             case SK_CX0:
               for (int j = 0; j < NV; ++j)
                 if (!(j & (1 << g.a)) && (j & (1 << g.b))) std::swap(v[j], v[j | (1 << g.a)]);
@@ -340,6 +365,44 @@ int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int3
   if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
   for (const SwSweep& sw : plan.sweeps) emulate_sweep(state, plan, sw);
   for (const SwPerm& pm : plan.restore) emulate_permute(state, n, pm);
+  return (int32_t)plan.sweeps.size();
+}
+
+int32_t sc_debug_emulate_slots(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                               int32_t low_qubits, int32_t nr, double budget,
+                               const int64_t* slot_after, const int32_t* slot_qubit,
+                               int64_t n_slots, const uint8_t* paulis, double* state) {
+  if (!state || (n_slots > 0 && (!slot_after || !slot_qubit || !paulis)))
+    return fail(SC_EINVAL, "null argument");
+  std::vector<PGate> gates;
+  int64_t next = 0;
+  for (int64_t i = 0; i < n_ops; ++i) {
+    PGate g;
+    bool produced = false;
+    if (!normalise_op(ops[i], nullptr, 0, &g, &produced))
+      return fail(SC_EINVAL, "op %lld: cannot normalise", (long long)i);
+    if (produced) {
+      g.op_index = i;
+      gates.push_back(g);
+    }
+    for (; next < n_slots && slot_after[next] == i; ++next) {
+      if (slot_qubit[next] < 0 || slot_qubit[next] >= n || paulis[next] > 3)
+        return fail(SC_EINVAL, "slot %lld: bad qubit or Pauli", (long long)next);
+      PGate sg;
+      std::memset(&sg, 0, sizeof sg);
+      sg.kind = PK_PAULI;
+      sg.q0 = slot_qubit[next];
+      sg.q1 = (int32_t)next;
+      sg.op_index = i;
+      gates.push_back(sg);
+    }
+  }
+  if (next != n_slots) return fail(SC_EINVAL, "slot_after must be sorted op indices");
+  PlanParams pp = debug_params(tile_qubits, low_qubits, nr, budget);
+  pp.relayout = false;
+  Plan plan = plan_sweeps(gates, n, pp);
+  if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+  for (const SwSweep& sw : plan.sweeps) emulate_sweep(state, plan, sw, paulis);
   return (int32_t)plan.sweeps.size();
 }
 

@@ -68,6 +68,9 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        registers (a fixed register permutation).
 // SK_PAULI: Pauli slot on register bit a; b = slot, the Pauli of each trajectory
 //        comes from the sweep's choice table (0 = I, 1 = X, 2 = Y, 3 = Z).
+// SK_PAULIF: a Pauli slot conjugated through register permutations folded into the
+//        stage's exit permutation; pool (u, w, p) for X, Y, Z in turn: the slot
+//        applies i^p X^u Z^w over the register bits (u, w bit masks).
 // SK_G1ALLQ: SK_G1ALL in rotation form: each 2x2 unitary is s_g * diag(1, e^{i phi})
 //        [[1, -t], [t, 1]] diag(1, e^{i lam}).  Pool: t of each of the K gates, then
 //        the products of their e^{i lam} and of their e^{i phi} over every non-empty
@@ -82,7 +85,7 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        bits (1 = X, 2 = Y, 3 = Z), b = gradient slot (the adjoint reverse sweep).
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are

@@ -11,6 +11,7 @@ import pytest
 import randcirc as RCirc
 from oracle import oracle as O
 from statecraft_b200 import _abi as A
+from statecraft_b200 import quantum as Q
 from statecraft_b200.engine import serialize_circuit
 
 HEADER = Path(__file__).resolve().parents[1] / "include" / "statecraft_b200.h"
@@ -237,3 +238,69 @@ def test_stage_peephole_matches_oracle(cfg, peephole, monkeypatch):
     init = RCirc.random_state(17, 17)
     got, _ = _emulate(c, init, *cfg)
     np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
+
+
+def _with_slots(c, slots, paulis):
+    """c with Pauli gates inserted after the ops named by slots (op index, qubit)."""
+    gate = {1: Q.PauliX(), 2: Q.PauliY(), 3: Q.PauliZ()}
+    out = Q.QuantumCircuit(c.qubitCount)
+    k = 0
+    for i, op in enumerate(c.operations):
+        out = out._append(op)
+        while k < len(slots) and slots[k][0] == i:
+            if paulis[k]:
+                out = out.append(gate[int(paulis[k])], slots[k][1])
+            k += 1
+    return out
+
+
+def _emulate_slots(c, slots, paulis, state, tile, low, nr, budget):
+    ops, n_ops = serialize_circuit(c)
+    after = np.array([s[0] for s in slots], dtype=np.int64)
+    qubit = np.array([s[1] for s in slots], dtype=np.int32)
+    codes = np.ascontiguousarray(paulis, dtype=np.uint8)
+    st = state.copy()
+    rc = A.load().sc_debug_emulate_slots(
+        c.qubitCount, ops, n_ops, tile, low, nr, budget,
+        after.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        qubit.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), len(slots),
+        codes.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+        st.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert rc >= 0, A.load().sc_last_error()
+    return st
+
+
+def _ghz_chain(n, seed):
+    from statecraft_b200 import workloads as W
+
+    rng = np.random.default_rng(seed)
+    c = W.ghz_circuit(n)
+    for _ in range(3):  # more CNOT layers, mixed with rotations, as register permutations
+        for q in rng.permutation(n - 1):
+            c = c.append(Q.CnotGate.of(), int(q), int(q) + 1)
+        c = c.append(RCirc.random_gate(rng), int(rng.integers(0, n)))
+        c = c.appendSwap(int(rng.integers(0, n // 2)), int(rng.integers(n // 2, n)))
+    return c
+
+
+@pytest.mark.parametrize("peephole", ["1", "0"])
+@pytest.mark.parametrize("cfg", [(11, 4, 4, -1.0), (10, 4, 3, -1.0), (9, 3, 2, 24.0)])
+def test_pauli_slots_through_folded_permutations(cfg, peephole, monkeypatch):
+    # noise slots after every op on each qubit it touches: CNOT chains fold into the
+    # stage exit permutation and the slots after them are conjugated (X -> X^u,
+    # Z -> +-Z^w, Y -> i X^u Z^w); one trajectory of every Pauli pattern mix
+    monkeypatch.setenv("STATECRAFT_B200_PEEPHOLE", peephole)
+    for n, seed in ((6, 1), (13, 2), (15, 3)):
+        c = _ghz_chain(n, seed) if seed != 2 else RCirc.random_circuit(n, 60, seed=77)
+        slots = []
+        for i, op in enumerate(c.operations):
+            for q in sorted(set(op.qubits_touched())):
+                slots.append((i, int(q)))
+        rng = np.random.default_rng(seed)
+        init = RCirc.random_state(n, seed)
+        for density in (0.05, 0.5):
+            paulis = np.where(rng.random(len(slots)) < density,
+                              rng.integers(1, 4, len(slots)), 0).astype(np.uint8)
+            got = _emulate_slots(c, slots, paulis, init, *cfg)
+            want = _oracle(_with_slots(c, slots, paulis), init)
+            np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
