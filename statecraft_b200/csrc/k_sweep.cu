@@ -34,9 +34,38 @@ namespace sc {
 
 namespace {
 
+// Tile offsets of a stage's registers: register j sits at local index l0 | off[j],
+// off[j] the OR of rb[k] (1 << register position k) over the set bits k of j.
+// Kept as NR words, not 2^NR, so the record loop carries fewer registers.
+template <int NR>
+struct RegOff {
+  uint32_t rb[NR];
+  __device__ __forceinline__ uint32_t operator[](int j) const {
+    uint32_t o = 0;
+#pragma unroll
+    for (int k = 0; k < NR; ++k)
+      if (j & (1 << k)) o |= rb[k];
+    return o;
+  }
+};
+
+// Exit-slot flips of a stage's slot folds: register j leaves through its slot XOR
+// x0 XOR (xc[k] for each set bit k of j); the flips are linear in j.
+template <int NR>
+struct SlotFlips {
+  uint32_t x0, xc[NR];
+  __device__ __forceinline__ uint32_t operator[](int j) const {
+    uint32_t f = x0;
+#pragma unroll
+    for (int k = 0; k < NR; ++k)
+      if (j & (1 << k)) f ^= xc[k];
+    return f;
+  }
+};
+
 template <typename R, int NR, int A_>
 __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R* m,
-                                   uint32_t l0, const uint32_t (&off)[1 << NR], uint32_t lmask) {
+                                   uint32_t l0, const RegOff<NR>& off, uint32_t lmask) {
   const R m00r = m[0], m00i = m[1], m01r = m[2], m01i = m[3];
   const R m10r = m[4], m10i = m[5], m11r = m[6], m11i = m[7];
 #pragma unroll
@@ -67,7 +96,7 @@ __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R*
 
 template <typename R, int NR, int A_>
 __device__ __forceinline__ void xswap(typename Amp<R>::type (&v)[1 << NR], uint32_t l0,
-                                      const uint32_t (&off)[1 << NR], uint32_t lmask) {
+                                      const RegOff<NR>& off, uint32_t lmask) {
   if (lmask == 0) {  // no control inside the tile: a plain register permutation
 #pragma unroll
     for (int j = 0; j < (1 << NR); ++j) {
@@ -166,7 +195,7 @@ __device__ __forceinline__ void rswap(typename Amp<R>::type (&v)[1 << NR]) {
 // diag1: diag(d0, d1) on one bit with tile-position controls lmask.
 template <typename R, int NR>
 __device__ __forceinline__ void diag1_any(typename Amp<R>::type (&v)[1 << NR], const R* m, int a,
-                                          uint32_t l0, const uint32_t (&off)[1 << NR],
+                                          uint32_t l0, const RegOff<NR>& off,
                                           uint32_t lmask, uint32_t base) {
   const uint32_t gb = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
   const int sh = a < 0 ? 0 : a;
@@ -184,7 +213,7 @@ __device__ __forceinline__ void diag1_any(typename Amp<R>::type (&v)[1 << NR], c
 // parity diagonal: factor d[bit(a) ^ bit(b)]
 template <typename R, int NR>
 __device__ __forceinline__ void diagp_any(typename Amp<R>::type (&v)[1 << NR], const R* m, int a,
-                                          int bq, uint32_t l0, const uint32_t (&off)[1 << NR],
+                                          int bq, uint32_t l0, const RegOff<NR>& off,
                                           uint32_t base) {
   const uint32_t gpar = (a < 0 ? ((base >> (-a - 1)) & 1u) : 0u) ^
                         (bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u);
@@ -200,7 +229,7 @@ __device__ __forceinline__ void diagp_any(typename Amp<R>::type (&v)[1 << NR], c
 // general two-bit diagonal, factor d[2 bit(a) + bit(b)]
 template <typename R, int NR>
 __device__ __forceinline__ void diag2_any(typename Amp<R>::type (&v)[1 << NR], const R* m, int a,
-                                          int bq, uint32_t l0, const uint32_t (&off)[1 << NR],
+                                          int bq, uint32_t l0, const RegOff<NR>& off,
                                           uint32_t base) {
   const uint32_t ga = a < 0 ? ((base >> (-a - 1)) & 1u) : 0u;
   const uint32_t gbb = bq < 0 ? ((base >> (-bq - 1)) & 1u) : 0u;
@@ -251,17 +280,14 @@ __device__ __forceinline__ void xswap0(typename Amp<R>::type (&v)[1 << NR]) {
 // by m = soff[1 << A_] (the offsets are linear in j); m = 0 where the gate's
 // controls outside the registers are not all set
 template <int NR, int A_>
-__device__ __forceinline__ void xfold(uint32_t (&sidx)[1 << NR], uint32_t m) {
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) sidx[j] ^= m;
+__device__ __forceinline__ void xfold(SlotFlips<NR>& fl, uint32_t m) {
+  fl.x0 ^= m;
 }
 
 // the same for X on register bit T_ controlled by register bit C_
 template <int NR, int T_, int C_>
-__device__ __forceinline__ void cxfold(uint32_t (&sidx)[1 << NR], uint32_t m) {
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j)
-    if (j & (1 << C_)) sidx[j] ^= m;
+__device__ __forceinline__ void cxfold(SlotFlips<NR>& fl, uint32_t m) {
+  fl.xc[C_] ^= m;
 }
 
 // controlled X, target register bit T_, control register bit C_, no other tile controls
@@ -340,7 +366,7 @@ __device__ __forceinline__ void g1allq(typename Amp<R>::type (&v)[1 << NR], cons
 // consecutive in the pool)
 template <typename R, int NR, int M>
 __device__ __forceinline__ void g1all(typename Amp<R>::type (&v)[1 << NR], const R* m,
-                                      uint32_t l0, const uint32_t (&off)[1 << NR]) {
+                                      uint32_t l0, const RegOff<NR>& off) {
   const R* mm = m;
   if constexpr ((M & 1) != 0) {
     g1<R, NR, 0>(v, mm, l0, off, 0u);
@@ -634,7 +660,9 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #pragma unroll
       for (int j = 0; j < NV; ++j) v[j] = cur[l0_first | tab.off[j]];
     }
-    uint32_t l0 = l0_first, off[NV], sidx[NV];
+    uint32_t l0 = l0_first, psw0 = 0;
+    RegOff<NR> off;
+    SlotFlips<NR> sidx;
 #pragma unroll 1
     for (int s = 0; s < ns; ++s) {
       const SwStage& stg = p.stages[s];
@@ -643,27 +671,42 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       const uint32_t sw0 = swz<R>(nl0);
       if (s > 0) {
         __syncthreads();  // readers of the buffer are done
-        // sidx: the previous stage's exit slots (its folded permutation applied)
+        // the previous stage's exit slots: its folded permutation (wsoff) and
+        // slot folds (sidx) applied
+        const SwStageTab& ptab = p.tabs[s - 1];
 #pragma unroll
-        for (int j = 0; j < NV; ++j) cur[sidx[j]] = v[j];
+        for (int j = 0; j < NV; ++j) cur[psw0 ^ ptab.wsoff[j] ^ sidx[j]] = v[j];
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < NV; ++j) v[j] = cur[sw0 ^ tab.soff[j]];
       }
+      psw0 = sw0;
+      sidx.x0 = 0u;
 #pragma unroll
-      for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.wsoff[j];
+      for (int k = 0; k < NR; ++k) sidx.xc[k] = 0u;
       l0 = nl0;
 #pragma unroll
-      for (int j = 0; j < NV; ++j) off[j] = tab.off[j];
+      for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
 
 #pragma unroll 1
-      for (int gi = stg.g0; gi < stg.g1; ++gi) {
-        const SwGate& g = p.gates[gi];
-        if (((uint64_t)base & g.gmask) != g.gmask) continue;
+      for (int gi = stg.g0;; ++gi) {
         if constexpr (kBatch) {
-          // identity Pauli (the common branch): skip the record before the jump
-          if ((g.kind == SK_PAULI || g.kind == SK_PAULIF) && codes[g.b] == 0) continue;
+          // the next record to apply: the records a trajectory skips (mostly the
+          // identity choice of a Pauli slot) go by in a scan of their own, off the
+          // loop edge that carries the amplitude registers
+#pragma unroll 1
+          for (; gi < stg.g1; ++gi) {
+            const SwGate& q = p.gates[gi];
+            if (((uint64_t)base & q.gmask) != q.gmask) continue;
+            if ((q.kind == SK_PAULI || q.kind == SK_PAULIF) && codes[q.b] == 0) continue;
+            break;
+          }
+          if (gi >= stg.g1) break;
+        } else {
+          if (gi >= stg.g1) break;
+          if (((uint64_t)base & p.gates[gi].gmask) != p.gates[gi].gmask) continue;
         }
+        const SwGate& g = p.gates[gi];
         const R* m = p.pool + g.moff;
         const uint32_t lmask = g.lmask;
         switch (g.code) {
@@ -805,7 +848,7 @@ template <typename R, int NR>
 __device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 << NR],
                                                   typename Amp<R>::type (&w)[1 << NR],
                                                   const SwGate& g, const R* m, uint32_t l0,
-                                                  const uint32_t (&off)[1 << NR], uint32_t base) {
+                                                  const RegOff<NR>& off, uint32_t base) {
   const uint32_t lmask = g.lmask;
   switch (g.code) {
 #define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask), g1<R, NR, A>(w, m, l0, off, lmask)
@@ -917,7 +960,8 @@ __global__ void __launch_bounds__(256, 2)
       v[j] = psi[base | gt_first | p.gfirst[j]];
       w[j] = lam[base | gt_first | p.gfirst[j]];
     }
-    uint32_t l0 = l0_first, off[NV], sidx[NV];
+    uint32_t l0 = l0_first, sidx[NV];
+    RegOff<NR> off;
 #pragma unroll 1
     for (int s = 0; s < ns; ++s) {
       const SwStage& stg = p.stages[s];
@@ -942,7 +986,7 @@ __global__ void __launch_bounds__(256, 2)
       for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.wsoff[j];
       l0 = nl0;
 #pragma unroll
-      for (int j = 0; j < NV; ++j) off[j] = tab.off[j];
+      for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
 #pragma unroll 1
       for (int gi = stg.g0; gi < stg.g1; ++gi) {
         const SwGate& g = p.gates[gi];
