@@ -73,6 +73,30 @@ def test_random_circuits_with_pauli_noise(ctx):
             np.testing.assert_allclose(res.states[t], want, rtol=0, atol=1e-12)
 
 
+def test_permutation_ladders_with_dense_noise(ctx):
+    # CNOT ladders and swaps fold into the stage exit permutations and the Pauli
+    # slots after them run conjugated (i^p X^u Z^w); heavy noise so most slots in
+    # most trajectories take an X, Y or Z branch
+    from statecraft_b200 import quantum as Q
+
+    n = 14
+    rng = np.random.default_rng(14)
+    c = W.ghz_circuit(n)
+    for _ in range(3):
+        for q in rng.permutation(n - 1):
+            c = c.append(Q.CnotGate.of(), int(q), int(q) + 1)
+        c = c.appendSwap(int(rng.integers(0, n // 2)), int(rng.integers(n // 2, n)))
+        c = c.append(RCirc.random_gate(rng), int(rng.integers(0, n)))
+    rec = touched_qubit_depolarizing(c, 0.5)
+    res = run_trajectories(c, rec, 8, noise_seed=4242, shots=0, measure_seed=0,
+                           return_states=True, context=ctx)
+    for t in range(8):
+        want, chosen = _oracle_trajectory(c, rec, 4242 + t)
+        np.testing.assert_array_equal(res.choices[t], chosen)
+        np.testing.assert_allclose(res.states[t], want, rtol=0, atol=1e-12)
+    assert np.count_nonzero(res.choices) > len(rec) * 8 // 4
+
+
 def test_complex64_trajectories(ctx64):
     c = W.ghz_circuit(10)
     rec = touched_qubit_depolarizing(c, 0.2)
