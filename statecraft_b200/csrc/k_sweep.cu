@@ -960,7 +960,7 @@ __global__ void __launch_bounds__(256, 2)
       v[j] = psi[base | gt_first | p.gfirst[j]];
       w[j] = lam[base | gt_first | p.gfirst[j]];
     }
-    uint32_t l0 = l0_first, sidx[NV];
+    uint32_t l0 = l0_first, psw0 = 0;
     RegOff<NR> off;
 #pragma unroll 1
     for (int s = 0; s < ns; ++s) {
@@ -970,10 +970,12 @@ __global__ void __launch_bounds__(256, 2)
       const uint32_t sw0 = swz<R>(nl0);
       if (s > 0) {
         __syncthreads();  // readers of the buffers are done
+        // the previous stage's exit slots (its folded permutation applied)
+        const SwStageTab& ptab = p.tabs[s - 1];
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
-          bp[sidx[j]] = v[j];
-          bl[sidx[j]] = w[j];
+          bp[psw0 ^ ptab.wsoff[j]] = v[j];
+          bl[psw0 ^ ptab.wsoff[j]] = w[j];
         }
         __syncthreads();
 #pragma unroll
@@ -982,8 +984,7 @@ __global__ void __launch_bounds__(256, 2)
           w[j] = bl[sw0 ^ tab.soff[j]];
         }
       }
-#pragma unroll
-      for (int j = 0; j < NV; ++j) sidx[j] = sw0 ^ tab.wsoff[j];
+      psw0 = sw0;
       l0 = nl0;
 #pragma unroll
       for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
