@@ -304,3 +304,15 @@ def test_pauli_slots_through_folded_permutations(cfg, peephole, monkeypatch):
             got = _emulate_slots(c, slots, paulis, init, *cfg)
             want = _oracle(_with_slots(c, slots, paulis), init)
             np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("cfg", [(11, 4, 4, -1.0), (10, 4, 3, -1.0), (8, 3, 2, 24.0)])
+def test_overlapping_permutation_folds(cfg, monkeypatch):
+    # runs of CNOTs and swaps on the same register bits: folded permutations that
+    # overlap compose into the exit permutation in time order
+    monkeypatch.setenv("STATECRAFT_B200_PEEPHOLE", "1")
+    for n, seed in ((9, 5), (14, 6), (16, 7)):
+        c = RCirc.random_circuit(n, 120, seed=seed, kinds=["cnot", "cnot", "swap", "single"])
+        init = RCirc.random_state(n, seed)
+        got, _ = _emulate(c, init, *cfg)
+        np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
