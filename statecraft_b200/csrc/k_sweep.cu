@@ -63,6 +63,18 @@ struct SlotFlips {
   }
 };
 
+// Slot of tile index i in the shared-memory layout a stage reads (its exchange's
+// swizzle; the fixed default unless rows[0] bit 15 is set).  Uniform per stage.
+template <typename R>
+__device__ __forceinline__ uint32_t stage_swz(uint32_t i, const SwStageTab& t) {
+  constexpr int K = Amp<R>::kSwizzleShift;
+  if (!(t.rows[0] & 0x8000u)) return swz<R>(i);
+  uint32_t lo = 0;
+#pragma unroll
+  for (int k = 0; k < K; ++k) lo |= (__popc(i & (uint32_t)t.rows[k]) & 1u) << k;
+  return i ^ lo;
+}
+
 template <typename R, int NR, int A_>
 __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R* m,
                                    uint32_t l0, const RegOff<NR>& off, uint32_t lmask) {
@@ -668,19 +680,20 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       const SwStage& stg = p.stages[s];
       const SwStageTab& tab = p.tabs[s];
       const uint32_t nl0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
-      const uint32_t sw0 = swz<R>(nl0);
       if (s > 0) {
         __syncthreads();  // readers of the buffer are done
         // the previous stage's exit slots: its folded permutation (wsoff) and
-        // slot folds (sidx) applied
+        // slot folds (sidx) applied, in this stage's layout
         const SwStageTab& ptab = p.tabs[s - 1];
 #pragma unroll
         for (int j = 0; j < NV; ++j) cur[psw0 ^ ptab.wsoff[j] ^ sidx[j]] = v[j];
         __syncthreads();
+        const uint32_t sw0 = stage_swz<R>(nl0, tab);
 #pragma unroll
         for (int j = 0; j < NV; ++j) v[j] = cur[sw0 ^ tab.soff[j]];
       }
-      psw0 = sw0;
+      // this stage's exit slots are in the next stage's layout
+      psw0 = s + 1 < ns ? stage_swz<R>(nl0, p.tabs[s + 1]) : 0u;
       sidx.x0 = 0u;
 #pragma unroll
       for (int k = 0; k < NR; ++k) sidx.xc[k] = 0u;
@@ -724,9 +737,9 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
     pauli<R, NR, A>(v, (uint32_t)codes[g.b]); \
   }
 #define SC_DO_XF(A) \
-  xfold<NR, A>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.soff[1 << (A)] : 0u)
+  xfold<NR, A>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
 #define SC_DO_CXF(A, B) \
-  cxfold<NR, A, B>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.soff[1 << (A)] : 0u)
+  cxfold<NR, A, B>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
           SC_CASES_1(SK_X0, SC_DO_X0)
           SC_CASES_2(SK_CX0, SC_DO_CX0)
           SC_CASES_1(SK_XF, SC_DO_XF)
@@ -1119,12 +1132,106 @@ uint32_t host_spread_out(uint32_t x, const SwSweep& sw) {
   return g;
 }
 
-uint32_t host_swz(uint32_t i, int shift) { return i ^ ((i >> shift) & ((1u << shift) - 1u)); }
+// An exchange swizzle (SwStageTab::rows): slot(i) = i ^ sum_k parity(i & rows[k]) << k.
+struct ExchangeSwizzle {
+  uint16_t rows[4];
+  bool general;
+};
+
+uint32_t apply_swizzle(uint32_t i, const ExchangeSwizzle& z, int K) {
+  uint32_t lo = 0;
+  for (int k = 0; k < K; ++k) lo |= (uint32_t)(__builtin_popcount(i & z.rows[k]) & 1) << k;
+  return i ^ lo;
+}
+
+// Tile positions of thread-index bits 0..K-1 in a stage: the threads whose accesses
+// share one 128-byte shared-memory wavefront differ in exactly these positions.
+void wavefront_positions(const SwStage& st, int nr, int K, int* pos) {
+  for (int b = 0; b < K; ++b) {
+    uint32_t x = 1u << b;
+    for (int k = 0; k < nr; ++k) x = insert_zero32(x, st.R[k]);
+    pos[b] = __builtin_ctz(x);
+  }
+}
+
+// The swizzle of one exchange: the K slot-bit vectors of the writer's wavefront
+// positions (pw) must be linearly independent over GF(2) (K distinct bank groups),
+// and so must the reader's (pr).  Position p < K contributes the unit vector of bit
+// p, position p >= K its column col[p] (bit k of col[p] = bit p of rows[k]).  The
+// default columns (col[K + k] = 1 << k) are kept when they serve both sides;
+// otherwise the columns of the wavefront positions >= K are searched.
+ExchangeSwizzle exchange_swizzle(const int* pw, const int* pr, int K, int T) {
+  int col[16] = {0};
+  auto set_default = [&]() {
+    for (int p = 0; p < 16; ++p) col[p] = (p >= K && p < 2 * K && p < T) ? 1 << (p - K) : 0;
+  };
+  set_default();
+  auto vec = [&](int p) { return p < K ? 1 << p : col[p]; };
+  // independence of the vectors of ps whose position is decided (< K, or in `fixed`)
+  auto independent = [&](const int* ps, uint32_t fixed) {
+    uint32_t span = 1u;  // bit u set: vector u lies in the span
+    for (int b = 0; b < K; ++b) {
+      if (ps[b] >= K && !((fixed >> ps[b]) & 1u)) continue;
+      const int v = vec(ps[b]);
+      if ((span >> v) & 1u) return false;
+      uint32_t nspan = span;
+      for (int u = 0; u < (1 << K); ++u)
+        if ((span >> u) & 1u) nspan |= 1u << (u ^ v);
+      span = nspan;
+    }
+    return true;
+  };
+  ExchangeSwizzle z{};
+  const bool fits = K <= 4 && T <= 15;
+  bool ok = fits && independent(pw, 0xffffu) && independent(pr, 0xffffu);
+  if (!ok && fits) {
+    int q[8], nq = 0;
+    for (int side = 0; side < 2; ++side)
+      for (int b = 0; b < K; ++b) {
+        const int p = side ? pr[b] : pw[b];
+        bool seen = p < K;
+        for (int i = 0; i < nq; ++i) seen = seen || q[i] == p;
+        if (!seen) q[nq++] = p;
+      }
+    // depth-first over the columns of q, pruned on the decided positions
+    int choice[8] = {0};
+    int i = 0;
+    uint32_t fixed = 0;
+    long budget = 1L << 20;
+    while (i >= 0 && budget-- > 0) {
+      if (i == nq) {
+        ok = true;
+        break;
+      }
+      if (++choice[i] >= (1 << K)) {  // exhausted: back up
+        choice[i] = 0;
+        fixed &= ~(1u << q[i]);
+        --i;
+        continue;
+      }
+      col[q[i]] = choice[i];
+      fixed |= 1u << q[i];
+      if (independent(pw, fixed) && independent(pr, fixed)) ++i;
+    }
+    z.general = ok;
+    if (!ok) set_default();  // the default is correct, only with bank conflicts
+  }
+  for (int k = 0; k < 4; ++k) {
+    z.rows[k] = 0;
+    if (k < K)
+      for (int p = K; p < T && p < 15; ++p)
+        if ((col[p] >> k) & 1) z.rows[k] |= (uint16_t)(1u << p);
+  }
+  if (z.general) z.rows[0] |= 0x8000u;
+  return z;
+}
 
 // Copies sweep `k` of `plan` into the kernel-parameter form (sweep-local indices,
 // per-stage register tables).
+// exchange_swizzles: give each exchange its own conflict-free swizzle (the fused
+// sweep kernel); false keeps the fixed swizzle (the adjoint kernel).
 template <typename R>
-bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
+bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_swizzles = true) {
   const SwSweep& sw = plan.sweeps[k];
   const int ns = sw.s1 - sw.s0;
   if (ns < 1 || ns > kSweepMaxStages || sw.nr > SW_MAX_NR) return false;
@@ -1153,25 +1260,46 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p) {
     p->hs[q] = sw.hs[q];
   }
   for (int q = 0; q < 32; ++q) p->outp[q] = (uint8_t)sw.outp[q];
-  const int shift = Amp<R>::kSwizzleShift;
+  const int K = Amp<R>::kSwizzleShift;
   const int nv = 1 << sw.nr;
+  // the swizzle of the layout each stage reads (stage 0 reads the linear layout)
+  std::vector<ExchangeSwizzle> zin(ns);
+  {
+    const int low[4] = {0, 1, 2, 3};
+    const ExchangeSwizzle dflt = exchange_swizzle(low, low, K, sw.T);
+    for (int s = 0; s < ns; ++s) zin[s] = dflt;
+    if (exchange_swizzles && sw.T - sw.nr >= K) {
+      for (int s = 1; s < ns; ++s) {
+        int pw[4], pr[4];
+        wavefront_positions(plan.stages[sw.s0 + s - 1], sw.nr, K, pw);
+        wavefront_positions(plan.stages[sw.s0 + s], sw.nr, K, pr);
+        zin[s] = exchange_swizzle(pw, pr, K, sw.T);
+      }
+    }
+  }
   for (int s = 0; s < ns; ++s) {
     SwStage st = plan.stages[sw.s0 + s];
     st.g0 -= g_lo;
     st.g1 -= g_lo;
     p->stages[s] = st;
+    const ExchangeSwizzle& zout = zin[s + 1 < ns ? s + 1 : s];
+    for (int b = 0; b < 4; ++b) {
+      p->tabs[s].rows[b] = zin[s].rows[b];
+      p->tabs[s].xoff[b] =
+          b < sw.nr ? (uint16_t)apply_swizzle(1u << st.R[b], zout, K) : (uint16_t)0;
+    }
     for (int j = 0; j < 16; ++j) {
       uint32_t o = 0;
       if (j < nv)
         for (int b = 0; b < sw.nr; ++b)
           if (j & (1 << b)) o |= 1u << st.R[b];
       p->tabs[s].off[j] = (uint16_t)o;
-      p->tabs[s].soff[j] = (uint16_t)host_swz(o, shift);
+      p->tabs[s].soff[j] = (uint16_t)apply_swizzle(o, zin[s], K);
     }
     for (int j = 0; j < 16; ++j) {
       const int pj = (j < nv) ? st.perm[j] : j;
       if (pj < 0 || pj >= 16) return false;
-      p->tabs[s].wsoff[j] = p->tabs[s].soff[pj];
+      p->tabs[s].wsoff[j] = (uint16_t)apply_swizzle(p->tabs[s].off[pj], zout, K);
     }
   }
   // slot folds act on the exchange slots: none may sit in the last stage
@@ -1266,7 +1394,7 @@ cudaError_t launch_adjoint_t(void* psi, void* lam, const Plan& plan, size_t k, d
                              int max_ctas, double* grad, int sm_count, cudaStream_t s) {
   using A = typename Amp<R>::type;
   SweepParams<R> p;
-  if (!fill_params(plan, k, &p) || p.nr != 3) return cudaErrorInvalidValue;
+  if (!fill_params(plan, k, &p, false) || p.nr != 3) return cudaErrorInvalidValue;
   // probe records carry the gradient slot; the kernel wants the local probe index
   ProbeSlots slots;
   int n_probes = 0;

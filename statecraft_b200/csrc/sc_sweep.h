@@ -13,13 +13,21 @@ constexpr int kSweepMaxGates = 78;   // stages <= gates + 2
 constexpr int kSweepMaxPool = 2048;  // matrix reals
 
 // Per-stage register tables computed on the host: off[j] is the tile offset of
-// register j (the OR of 1 << R[k] over the set bits k of j), soff[j] its swizzled
-// shared-memory slot (the swizzle is XOR-linear over disjoint bits) and wsoff[j]
-// the slot register j is written to when the stage ends (soff[perm[j]]).
+// register j (the OR of 1 << R[k] over the set bits k of j), soff[j] its slot in
+// the shared-memory layout the stage reads, wsoff[j] the slot register j is written
+// to when the stage ends (register perm[j] in the next stage's layout) and xoff[a]
+// the offset of register bit a in that layout (slot folds).  Each exchange between
+// two stages has its own XOR swizzle, slot(i) = i ^ sum_k parity(i & rows[k]) << k
+// over the low K slot bits (K = log2 of the amplitudes per 128-byte row); rows[]
+// only read bits >= K, so every swizzle is a bijection and XOR-linear over disjoint
+// bits.  rows[] here is the swizzle of the layout this stage reads; bit 15 of
+// rows[0] marks one that differs from the fixed default (rows[k] = 1 << (K + k)).
 struct SwStageTab {
   uint16_t off[16];
   uint16_t soff[16];
   uint16_t wsoff[16];
+  uint16_t xoff[4];
+  uint16_t rows[4];
 };
 
 template <typename R>
