@@ -248,6 +248,13 @@ SC_API int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, i
  * kernel's tile / stage / register semantics; returns the number of sweeps. */
 SC_API int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
                                 int32_t low_qubits, int32_t nr, double budget, double* state);
+/* Checks the shared-memory exchange tables the sweep kernel would get for the plan
+ * of ops (dtype SC_C64 or SC_C128): each exchange between two stages writes and reads
+ * every slot once and agrees on where each amplitude lies.  stats[4] = {exchanges,
+ * exchanges with their own swizzle, 128-byte wavefronts, wavefronts with a bank
+ * conflict}.  Returns the number of sweeps, or SC_ESTATE if a table is inconsistent. */
+SC_API int32_t sc_debug_check_exchanges(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                                 int32_t low_qubits, int32_t nr, int32_t dtype, int64_t* stats);
 /* As sc_debug_emulate_sweeps for one trajectory of a batch: Pauli slot j sits after
  * op slot_after[j] (non-decreasing) on qubit slot_qubit[j] and applies paulis[j]
  * (0 = I, 1 = X, 2 = Y, 3 = Z), planned the way sc_trajectories plans slots. */

@@ -148,6 +148,9 @@ SIGNATURES = {
     "sc_debug_emulate_sweeps": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                                  ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                  ctypes.c_double, _P(ctypes.c_double)]),
+    "sc_debug_check_exchanges": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
+                                                  ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                                  ctypes.c_int32, _P(ctypes.c_int64)]),
     "sc_debug_emulate_slots": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                                 ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_double, _P(ctypes.c_int64),

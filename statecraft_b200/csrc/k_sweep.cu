@@ -23,6 +23,7 @@
 // CTA records an error in `err`, waits (bounded) for the copies it issued and
 // returns, and the host reports SC_ETIMEOUT.
 #include <algorithm>
+#include <memory>
 #include <mutex>
 #include <type_traits>
 
@@ -1154,13 +1155,14 @@ void wavefront_positions(const SwStage& st, int nr, int K, int* pos) {
   }
 }
 
-// The swizzle of one exchange: the K slot-bit vectors of the writer's wavefront
-// positions (pw) must be linearly independent over GF(2) (K distinct bank groups),
-// and so must the reader's (pr).  Position p < K contributes the unit vector of bit
+// The swizzle of one exchange: the slot-bit vectors of the writer's m wavefront
+// positions (pw; m = K, or the thread bits of a tile with fewer threads than a
+// wavefront) must be linearly independent over GF(2) (distinct bank groups), and so
+// must the reader's (pr).  Position p < K contributes the unit vector of bit
 // p, position p >= K its column col[p] (bit k of col[p] = bit p of rows[k]).  The
 // default columns (col[K + k] = 1 << k) are kept when they serve both sides;
 // otherwise the columns of the wavefront positions >= K are searched.
-ExchangeSwizzle exchange_swizzle(const int* pw, const int* pr, int K, int T) {
+ExchangeSwizzle exchange_swizzle(const int* pw, const int* pr, int m, int K, int T) {
   int col[16] = {0};
   auto set_default = [&]() {
     for (int p = 0; p < 16; ++p) col[p] = (p >= K && p < 2 * K && p < T) ? 1 << (p - K) : 0;
@@ -1170,7 +1172,7 @@ ExchangeSwizzle exchange_swizzle(const int* pw, const int* pr, int K, int T) {
   // independence of the vectors of ps whose position is decided (< K, or in `fixed`)
   auto independent = [&](const int* ps, uint32_t fixed) {
     uint32_t span = 1u;  // bit u set: vector u lies in the span
-    for (int b = 0; b < K; ++b) {
+    for (int b = 0; b < m; ++b) {
       if (ps[b] >= K && !((fixed >> ps[b]) & 1u)) continue;
       const int v = vec(ps[b]);
       if ((span >> v) & 1u) return false;
@@ -1187,7 +1189,7 @@ ExchangeSwizzle exchange_swizzle(const int* pw, const int* pr, int K, int T) {
   if (!ok && fits) {
     int q[8], nq = 0;
     for (int side = 0; side < 2; ++side)
-      for (int b = 0; b < K; ++b) {
+      for (int b = 0; b < m; ++b) {
         const int p = side ? pr[b] : pw[b];
         bool seen = p < K;
         for (int i = 0; i < nq; ++i) seen = seen || q[i] == p;
@@ -1266,14 +1268,15 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
   std::vector<ExchangeSwizzle> zin(ns);
   {
     const int low[4] = {0, 1, 2, 3};
-    const ExchangeSwizzle dflt = exchange_swizzle(low, low, K, sw.T);
+    const ExchangeSwizzle dflt = exchange_swizzle(low, low, K, K, sw.T);
     for (int s = 0; s < ns; ++s) zin[s] = dflt;
-    if (exchange_swizzles && sw.T - sw.nr >= K) {
+    const int m = std::min(K, sw.T - sw.nr);  // thread bits sharing one wavefront
+    if (exchange_swizzles && m > 0) {
       for (int s = 1; s < ns; ++s) {
         int pw[4], pr[4];
-        wavefront_positions(plan.stages[sw.s0 + s - 1], sw.nr, K, pw);
-        wavefront_positions(plan.stages[sw.s0 + s], sw.nr, K, pr);
-        zin[s] = exchange_swizzle(pw, pr, K, sw.T);
+        wavefront_positions(plan.stages[sw.s0 + s - 1], sw.nr, m, pw);
+        wavefront_positions(plan.stages[sw.s0 + s], sw.nr, m, pr);
+        zin[s] = exchange_swizzle(pw, pr, m, K, sw.T);
       }
     }
   }
@@ -1333,6 +1336,77 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
 }
 
 }  // namespace
+
+namespace {
+
+template <typename R>
+bool check_exchanges_t(const Plan& plan, int64_t* st) {
+  const int K = Amp<R>::kSwizzleShift;
+  // the kernel's slot map (stage_swz), restated on the host
+  auto slot_of = [&](uint32_t i, const SwStageTab& t) {
+    if (!(t.rows[0] & 0x8000u)) return i ^ ((i >> K) & ((1u << K) - 1u));
+    uint32_t lo = 0;
+    for (int k = 0; k < K; ++k) lo |= (uint32_t)(__builtin_popcount(i & t.rows[k]) & 1) << k;
+    return i ^ lo;
+  };
+  auto l0_of = [](uint32_t tid, const SwStage& s, int nr) {
+    for (int k = 0; k < nr; ++k) tid = insert_zero32(tid, s.R[k]);
+    return tid;
+  };
+  std::unique_ptr<SweepParams<R>> pp(new SweepParams<R>());
+  SweepParams<R>& p = *pp;
+  for (size_t k = 0; k < plan.sweeps.size(); ++k) {
+    if (!fill_params(plan, k, &p)) return false;
+    const int T = p.T, nr = p.nr, NV = 1 << nr, threads = 1 << (T - nr);
+    for (int s = 1; s < p.n_stages; ++s) {
+      ++st[0];
+      if (p.tabs[s].rows[0] & 0x8000u) ++st[1];
+      std::vector<int64_t> wslot((size_t)1 << T, -1), rslot((size_t)1 << T, -1);
+      const SwStage& sw = p.stages[s - 1];
+      const SwStage& sr = p.stages[s];
+      for (int tid = 0; tid < threads; ++tid) {
+        const uint32_t lw = l0_of(tid, sw, nr), lr = l0_of(tid, sr, nr);
+        const uint32_t bw = slot_of(lw, p.tabs[s]), br = slot_of(lr, p.tabs[s]);
+        for (int j = 0; j < NV; ++j) {
+          const uint32_t a = bw ^ p.tabs[s - 1].wsoff[j];  // register j leaves as perm[j]
+          const uint32_t b = br ^ p.tabs[s].soff[j];
+          if (a >= (1u << T) || b >= (1u << T) || wslot[a] >= 0 || rslot[b] >= 0) return false;
+          wslot[a] = lw | p.tabs[s - 1].off[sw.perm[j]];
+          rslot[b] = lr | p.tabs[s].off[j];
+        }
+        for (int a = 0; a < nr; ++a)
+          if (p.tabs[s - 1].xoff[a] != slot_of(1u << sw.R[a], p.tabs[s])) return false;
+      }
+      if (wslot != rslot) return false;
+      // wavefronts: 2^K consecutive threads (all of a smaller tile), one register
+      // index, each side
+      const int group = std::min(1 << K, threads);
+      for (int side = 0; side < 2; ++side)
+        for (int t0 = 0; t0 < threads; t0 += group)
+          for (int j = 0; j < NV; ++j) {
+            uint32_t seen = 0;
+            int n = 0;
+            for (int t = t0; t < t0 + group; ++t, ++n) {
+              const uint32_t a = side == 0
+                  ? slot_of(l0_of(t, sw, nr), p.tabs[s]) ^ p.tabs[s - 1].wsoff[j]
+                  : slot_of(l0_of(t, sr, nr), p.tabs[s]) ^ p.tabs[s].soff[j];
+              seen |= 1u << (a & ((1u << K) - 1u));
+            }
+            ++st[2];
+            if (__builtin_popcount(seen) < n) ++st[3];
+          }
+    }
+  }
+  return true;
+}
+
+}  // namespace
+
+bool check_exchange_tables(const Plan& plan, int dtype, int64_t* stats) {
+  for (int i = 0; i < 4; ++i) stats[i] = 0;
+  return dtype == SC_C64 ? check_exchanges_t<float>(plan, stats)
+                         : check_exchanges_t<double>(plan, stats);
+}
 
 cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int* err,
                          int sm_count, cudaStream_t s) {

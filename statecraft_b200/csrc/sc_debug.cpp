@@ -406,4 +406,20 @@ int32_t sc_debug_emulate_slots(int32_t n, const sc_op* ops, int64_t n_ops, int32
   return (int32_t)plan.sweeps.size();
 }
 
+int32_t sc_debug_check_exchanges(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                                 int32_t low_qubits, int32_t nr, int32_t dtype, int64_t* stats) {
+  std::vector<PGate> gates;
+  int rc = normalise_all(n, ops, n_ops, gates);
+  if (rc != SC_OK) return rc;
+  if (!stats) return fail(SC_EINVAL, "stats is null");
+  if (dtype != SC_C64 && dtype != SC_C128) return fail(SC_EINVAL, "dtype must be SC_C64 or SC_C128");
+  PlanParams pp = debug_params(tile_qubits, low_qubits, nr, -1.0);
+  pp.relayout = false;
+  Plan plan = plan_sweeps(gates, n, pp);
+  if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+  if (!check_exchange_tables(plan, dtype, stats))
+    return fail(SC_ESTATE, "inconsistent shared-memory exchange tables");
+  return (int32_t)plan.sweeps.size();
+}
+
 }  // extern "C"

@@ -237,6 +237,12 @@ cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, co
 // sweep k on psi and lambda and adds its probe sums to grad[slot] through
 // `partial` (room for max_ctas x kSweepMaxGates doubles).
 bool adjoint_plan_supported(const Plan& plan);
+// Host check of a plan's shared-memory exchange tables (the layouts the sweep kernel
+// uses): every exchange writes and reads each slot once, the slot a writer uses for
+// a tile index is the one the reader takes it from, and stats[] = {exchanges,
+// exchanges with a non-default swizzle, wavefronts, wavefronts with a bank
+// conflict}.  False when the tables are inconsistent or a sweep has no kernel form.
+bool check_exchange_tables(const Plan& plan, int dtype, int64_t* stats);
 cudaError_t launch_adjoint_sweep(int dtype, void* psi, void* lam, const Plan& plan, size_t k,
                                  double* partial, int max_ctas, double* grad, int sm_count,
                                  cudaStream_t s);

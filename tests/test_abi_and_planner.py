@@ -316,3 +316,27 @@ def test_overlapping_permutation_folds(cfg, monkeypatch):
         init = RCirc.random_state(n, seed)
         got, _ = _emulate(c, init, *cfg)
         np.testing.assert_allclose(got, _oracle(c, init), rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("dtype", [A.SC_C128, A.SC_C64])
+@pytest.mark.parametrize("nr", [4, 3])
+def test_exchange_tables_consistent_and_conflict_free(dtype, nr):
+    # the shared-memory tables the sweep kernel gets: per exchange, every slot written
+    # and read once, writer and reader agree on each amplitude's slot, and the
+    # per-exchange swizzle leaves no 128-byte wavefront with a bank conflict
+    from statecraft_b200 import workloads as W
+
+    low = 4 if dtype == A.SC_C128 else 5
+    circuits = [W.brickwall_circuit(26, 3, seed=26, mcz=True, rzz=True),
+                RCirc.random_circuit(18, 150, seed=5),
+                RCirc.random_circuit(14, 200, seed=9, kinds=["cnot", "swap", "single", "multi"])]
+    for c in circuits:
+        ops, n_ops = serialize_circuit(c)
+        stats = np.zeros(4, dtype=np.int64)
+        rc = A.load().sc_debug_check_exchanges(
+            c.qubitCount, ops, n_ops, 11, low, nr, dtype,
+            stats.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        assert rc > 0, A.load().sc_last_error()
+        exchanges, general, wavefronts, conflicted = stats.tolist()
+        assert exchanges > 0 and wavefronts > 0
+        assert conflicted == 0
