@@ -340,3 +340,27 @@ def test_exchange_tables_consistent_and_conflict_free(dtype, nr):
         exchanges, general, wavefronts, conflicted = stats.tolist()
         assert exchanges > 0 and wavefronts > 0
         assert conflicted == 0
+
+
+def test_exchange_tables_over_plan_shapes():
+    # tile sizes, register counts and low-qubit counts the planner accepts, small
+    # tiles (fewer threads than a wavefront) included: the tables stay consistent
+    # and conflict-free for every shape
+    checked = 0
+    for seed, n in ((0, 7), (1, 13)):
+        c = RCirc.random_circuit(n, 80, seed=100 * seed + n)
+        ops, n_ops = serialize_circuit(c)
+        for dtype in (A.SC_C128, A.SC_C64):
+            for tile in (6, 8, 11):
+                for nr in (2, 3, 4):
+                    for low in (3, 4):
+                        stats = np.zeros(4, dtype=np.int64)
+                        rc = A.load().sc_debug_check_exchanges(
+                            n, ops, n_ops, tile, low, nr, dtype,
+                            stats.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+                        if rc < 0:  # a shape the planner does not take
+                            assert b"inconsistent" not in (A.load().sc_last_error() or b"")
+                            continue
+                        assert stats[3] == 0, (n, dtype, tile, nr, low, stats.tolist())
+                        checked += int(stats[0] > 0)
+    assert checked >= 40
