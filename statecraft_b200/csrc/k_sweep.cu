@@ -1199,7 +1199,7 @@ ExchangeSwizzle exchange_swizzle(const int* pw, const int* pr, int m, int K, int
     int choice[8] = {0};
     int i = 0;
     uint32_t fixed = 0;
-    long budget = 1L << 20;
+    long budget = 1L << 16;  // bounds the planning time; the default stays correct
     while (i >= 0 && budget-- > 0) {
       if (i == nq) {
         ok = true;
