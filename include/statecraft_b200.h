@@ -220,18 +220,19 @@ SC_API void* sc_stream(void* ctx);
 SC_API int32_t sc_last_plan_stats(void* ctx, int64_t* sweeps, int64_t* gates, int64_t* stages);
 
 /* Sampling that allocates nothing.  No counterpart in the reference: it serves
- * callers that cannot call cudaMalloc when they sample -- code recording a CUDA
- * graph, frameworks whose device memory belongs to their own pool allocator, and
- * serving loops that must not allocate after start-up.  Samples every qubit of a
- * state the caller holds in device memory (d_state: 2^n amplitudes of `dtype`;
- * outcome = basis index) into the caller's device buffer d_outcomes[shots], on the
- * caller's cudaStream_t `stream`, and returns after the stream has finished.
+ * callers that cannot call cudaMalloc when they sample -- frameworks whose device
+ * memory belongs to their own pool allocator, serving loops that must not allocate
+ * after start-up, and processes that have already handed the GPU's memory to their
+ * own buffers.  Samples every qubit of a state the caller holds in device memory
+ * (d_state: 2^n amplitudes of `dtype`; outcome = basis index) into the caller's
+ * device buffer d_outcomes[shots], on the caller's cudaStream_t `stream`, and
+ * returns after the stream has finished.
  * Uniforms: d_uniforms[shot] (device, nullable) else SplittableRandom(seed).
  * Scratch is a fixed array in the library's device data sized for at most 2^30
  * amplitudes (30 qubits, about 8 MiB held by every GPU that loads the library);
  * larger states return SC_EINVAL.  The first call on a device looks the array up
- * (make it before any stream capture).  All calls share the array: calls that
- * overlap on the GPU race. */
+ * (make it before any stream capture); a cudaDeviceReset after that is not
+ * supported.  All calls share the array: calls that overlap on the GPU race. */
 SC_API int32_t sc_sample_static(const void* d_state, int32_t n_qubits, int32_t dtype,
                                 int64_t shots, uint64_t seed, const double* d_uniforms,
                                 int32_t* d_outcomes, void* stream);

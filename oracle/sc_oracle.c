@@ -454,6 +454,23 @@ EXPORT void scx_probabilities(const double* s, int n, const int32_t* qubits, int
                               double* probs) {
   const uint64_t dim = 1ULL << n;
   memset(probs, 0, sizeof(double) * ((size_t)1 << m));
+  uint64_t covered = 0;
+  for (int bit = 0; bit < m; ++bit) covered |= 1ULL << qubits[bit];
+  if (m == n && covered == dim - 1) {
+    /* every qubit measured once: each outcome receives exactly one basis state's p, so the
+     * loop has no accumulation order and runs in parallel with identical results */
+#pragma omp parallel for schedule(static)
+    for (int64_t basis = 0; basis < (int64_t)dim; ++basis) {
+      double ar = s[2 * basis], ai = s[2 * basis + 1];
+      double p = (ar * ar) + (ai * ai);
+      if (p == 0.0) continue;
+      uint64_t outcome = 0;
+      for (int bit = 0; bit < m; ++bit)
+        if (((uint64_t)basis >> qubits[bit]) & 1ULL) outcome |= (1ULL << bit);
+      probs[outcome] = p;
+    }
+    return;
+  }
   for (uint64_t basis = 0; basis < dim; ++basis) {
     double ar = s[2 * basis], ai = s[2 * basis + 1];
     double p = (ar * ar) + (ai * ai);

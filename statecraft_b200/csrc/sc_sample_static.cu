@@ -1,12 +1,12 @@
 // Sampling that allocates nothing.
 //
-// Who needs it: callers that cannot call cudaMalloc at the moment they sample.
-// A caller recording work into a CUDA graph cannot allocate inside the capture; a
+// Who needs it: callers that cannot call cudaMalloc at the moment they sample.  A
 // framework whose device memory is owned by its own pool allocator cannot let a
 // library take memory behind the pool's back; a serving loop that must not stall or
-// fail on an allocation after start-up cannot afford one per request.  They hold
-// the state vector in their own device memory and want outcomes written into their
-// own device buffer.
+// fail on an allocation after start-up cannot afford one per request; a process
+// that has handed almost all of the GPU's memory to its own buffers has nothing
+// left for a library to allocate.  They hold the state vector in their own device
+// memory and want outcomes written into their own device buffer.
 //
 // sc_sample_static samples every qubit of such a state (outcome = basis index, the
 // countsAll convention) with the same kernels as sc_sample.  Its only scratch, the
@@ -18,9 +18,12 @@
 // The array's name is a host-side stand-in in host code, so its device address is
 // looked up with cudaGetSymbolAddress once per device, with that device current,
 // on the first call made on it; make that first call before any stream capture.
+// The address is kept for the life of the process, so a cudaDeviceReset between
+// calls is not supported (the reset frees the module that holds the array).
 // Every call shares the array and it keeps the previous call's contents; the
 // kernels write every word they read earlier in the same call, so nothing needs
-// clearing, but calls that overlap on the GPU race on the array.
+// clearing, but calls that overlap on the GPU race on the array.  Each call waits
+// for its stream and reads a status word back before it returns.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -68,7 +71,8 @@ extern "C" int32_t sc_sample_static(const void* d_state, int32_t n_qubits, int32
   if (!d_state || !d_outcomes) return fail(SC_EINVAL, "state and outcome buffers are required");
   if (dtype != SC_C128 && dtype != SC_C64) return fail(SC_EINVAL, "dtype must be SC_C128 or SC_C64");
   if (n_qubits < 1) return fail(SC_EINVAL, "qubitCount must be positive");
-  if ((1ULL << n_qubits) > kStaticMaxAmps || n_qubits > 62)
+  // the qubit count is bounded before it is used as a shift
+  if (n_qubits > 30 || (1ULL << n_qubits) > kStaticMaxAmps)
     return fail(SC_EINVAL, "sc_sample_static supports states of up to 2^30 amplitudes (30 qubits), got %d qubits",
                 n_qubits);
   if (shots <= 0) return fail(SC_EINVAL, "shots must be positive");

@@ -1,12 +1,12 @@
 """sc_sample_static: sampling for callers that cannot allocate device memory.
 
-Callers recording a CUDA graph, frameworks that own all device memory through their
-own pool, and serving loops that forbid allocation after start-up hold the state in
-their own device memory; sc_sample_static samples it into their device buffer using
-a fixed scratch array inside the library.  Checked through the C ABI against the
-context sampler (sc_sample) on the same state and uniforms: outcomes are integers and
-must be identical, on two calls in a row.  This file is collected last so a failure
-here cannot hide the rest of the suite.
+Frameworks that own all device memory through their own pool, and serving loops
+that forbid allocation after start-up, hold the state in their own device memory;
+sc_sample_static samples it into their device buffer using a fixed scratch array
+inside the library.  Checked through the C ABI against the context sampler
+(sc_sample) on the same state and uniforms: outcomes are integers and must be
+identical, on two calls in a row.  This file is collected last so a failure here
+cannot hide the rest of the suite.
 """
 import ctypes
 
@@ -67,7 +67,9 @@ def test_static_sampler_matches_context_sampler(dtype):
 
 def test_static_sampler_rejects_oversized_state():
     lib = A.load()
-    rc = lib.sc_sample_static(ctypes.c_void_p(16), 31, A.SC_C128, 8, 1, None, ctypes.c_void_p(16),
-                              None)
-    assert rc == A.SC_EINVAL
-    assert b"2^30" in lib.sc_last_error()
+    # 31 qubits is one past the scratch size; 64 and 200 would overflow a shift
+    for n in (31, 64, 200):
+        rc = lib.sc_sample_static(ctypes.c_void_p(16), n, A.SC_C128, 8, 1, None,
+                                  ctypes.c_void_p(16), None)
+        assert rc == A.SC_EINVAL
+        assert b"2^30" in lib.sc_last_error()
