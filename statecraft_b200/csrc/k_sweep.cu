@@ -290,7 +290,7 @@ __device__ __forceinline__ void xswap0(typename Amp<R>::type (&v)[1 << NR]) {
 
 // X on register bit A_ applied to the stage's exit slots: the amplitude in register
 // j leaves through the slot of register j ^ (1 << A_), whose swizzled offset differs
-// by m = soff[1 << A_] (the offsets are linear in j); m = 0 where the gate's
+// by m = xoff[A_], the slot offset of that bit (the offsets are linear in j); m = 0 where the gate's
 // controls outside the registers are not all set
 template <int NR, int A_>
 __device__ __forceinline__ void xfold(SlotFlips<NR>& fl, uint32_t m) {
@@ -447,6 +447,22 @@ __device__ __forceinline__ void pauli_frame(typename Amp<R>::type (&v)[1 << NR],
   }
 }
 
+// X on the register bits of mask b (a rotation record's leading X, when it is not
+// folded into the stage's read)
+template <typename R, int NR>
+__device__ __forceinline__ void prex(typename Amp<R>::type (&v)[1 << NR], uint32_t b) {
+  if (b & 1u) xswap0<R, NR, 0>(v);
+  if constexpr (NR > 1) {
+    if (b & 2u) xswap0<R, NR, 1>(v);
+  }
+  if constexpr (NR > 2) {
+    if (b & 4u) xswap0<R, NR, 2>(v);
+  }
+  if constexpr (NR > 3) {
+    if (b & 8u) xswap0<R, NR, 3>(v);
+  }
+}
+
 // switch cases for the dispatch code (sw_code): one jump per gate into code that
 // is specialised on its register bits
 #define SC_CASE_1(K, A, F) \
@@ -504,6 +520,62 @@ __device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
 #pragma unroll 1
   for (int k = 0; k < p.h; ++k) base = insert_zero32(base, p.hs[k]);
   return base;
+}
+
+// End of a stage.  A stage before the last writes its registers to their slots in
+// the next stage's layout (folded permutation and slot folds applied).  The last
+// stage applies the sweep's scalar and stores the tile: to global memory (direct
+// path) or into the linear output layout of the tile buffer (bulk-store path).  Each
+// branch consumes the registers, so none of them is live past it.
+template <typename R, int NR, bool kTma>
+__device__ __forceinline__ void stage_exit(const typename Amp<R>::type (&v)[1 << NR], bool last,
+                                           typename Amp<R>::type* cur, uint32_t wbase,
+                                           const SwStageTab& tab, const SlotFlips<NR>& fl,
+                                           typename Amp<R>::type* __restrict__ dst,
+                                           uint32_t gt_last, uint32_t l0_last,
+                                           const SweepParams<R>& p) {
+  constexpr int NV = 1 << NR;
+  if (!last) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j) cur[wbase ^ tab.wsoff[j] ^ fl[j]] = v[j];
+    return;
+  }
+  if constexpr (kTma) {
+    if (p.has_scale) {
+#pragma unroll
+      for (int j = 0; j < NV; ++j) cur[l0_last | p.lastoff[j]] = cmul(p.scale_re, p.scale_im, v[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < NV; ++j) cur[l0_last | p.lastoff[j]] = v[j];
+    }
+  } else {
+    if (p.has_scale) {
+#pragma unroll
+      for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = cmul(p.scale_re, p.scale_im, v[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
+    }
+  }
+}
+
+// A stage whose only register record is one rotation-form record on the register
+// bits of M (M = 0: none): read, compute and exit as one piece of straight-line code.
+// The record's leading X, if any, is folded into tab.rd.
+template <typename R, int NR, int M, bool kTma>
+__device__ __forceinline__ void fast_stage(typename Amp<R>::type* cur, uint32_t rbase,
+                                           const SwStageTab& tab, const R* q, bool last,
+                                           uint32_t wbase, const SlotFlips<NR>& fl,
+                                           typename Amp<R>::type* __restrict__ dst,
+                                           uint32_t gt_last, uint32_t l0_last,
+                                           const SweepParams<R>& p) {
+  constexpr int NV = 1 << NR;
+  typename Amp<R>::type v[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
+  if constexpr (M != 0) g1allq<R, NR, M>(v, q);
+  if (!last || kTma) __syncthreads();  // every read of `cur` in this stage is done
+  stage_exit<R, NR, kTma>(v, last, cur, wbase, tab, fl, dst, gt_last, l0_last, p);
 }
 
 // Register cap of the complex128 NR = 3 variant: 96 registers let five 128-thread
@@ -612,10 +684,9 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   // of the next tile into the other buffer with cp.async while this tile computes
   auto prefetch_own = [&](uint32_t tt, A* dst) {
     const A* src = item_state(tt) + tile_base(tt & tile_mask, p);
-    const SwStageTab& tab0 = p.tabs[0];
 #pragma unroll
     for (int j = 0; j < NV; ++j)
-      cp_async<sizeof(A)>(dst + (l0_first | tab0.off[j]), src + (gt_first | p.gfirst[j]));
+      cp_async<sizeof(A)>(dst + (l0_first | p.off0[j]), src + (gt_first | p.gfirst[j]));
   };
 
   uint32_t t = blockIdx.x;
@@ -666,39 +737,67 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       }
     }
 
-    A v[NV];
-    {
-      // both paths stage the tile in `cur` in the linear layout
-      const SwStageTab& tab = p.tabs[0];
-#pragma unroll
-      for (int j = 0; j < NV; ++j) v[j] = cur[l0_first | tab.off[j]];
-    }
-    uint32_t l0 = l0_first, psw0 = 0;
-    RegOff<NR> off;
-    SlotFlips<NR> sidx;
+    A* const dst = item_state(t) + base;
 #pragma unroll 1
     for (int s = 0; s < ns; ++s) {
       const SwStage& stg = p.stages[s];
       const SwStageTab& tab = p.tabs[s];
-      const uint32_t nl0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
-      if (s > 0) {
-        __syncthreads();  // readers of the buffer are done
-        // the previous stage's exit slots: its folded permutation (wsoff) and
-        // slot folds (sidx) applied, in this stage's layout
-        const SwStageTab& ptab = p.tabs[s - 1];
-#pragma unroll
-        for (int j = 0; j < NV; ++j) cur[psw0 ^ ptab.wsoff[j] ^ sidx[j]] = v[j];
-        __syncthreads();
-        const uint32_t sw0 = stage_swz<R>(nl0, tab);
-#pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = cur[sw0 ^ tab.soff[j]];
-      }
-      // this stage's exit slots are in the next stage's layout
-      psw0 = s + 1 < ns ? stage_swz<R>(nl0, p.tabs[s + 1]) : 0u;
+      const bool last = s + 1 == ns;
+      const uint32_t l0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
+      // where this stage reads its registers and where it writes them for the next
+      const uint32_t rbase = (s == 0) ? l0_first : stage_swz<R>(l0, tab);
+      const uint32_t wbase = last ? 0u : stage_swz<R>(l0, p.tabs[s + 1]);
+      if (s > 0) __syncthreads();  // the previous stage's exit stores are visible
+      SlotFlips<NR> sidx;
       sidx.x0 = 0u;
 #pragma unroll
       for (int k = 0; k < NR; ++k) sidx.xc[k] = 0u;
-      l0 = nl0;
+      const int prog = tab.prog;
+      if (prog != kProgGeneric) {
+        // A stage with one rotation record: its other records are slot folds, which
+        // only change where registers leave (integer work, decided first); the
+        // registers then live in straight-line code from the read to the exit.
+#pragma unroll 1
+        for (int gi = stg.g0; gi < stg.g1; ++gi) {
+          const SwGate& g = p.gates[gi];
+          if (g.kind != SK_XF && g.kind != SK_CXF) continue;
+          if (((uint64_t)base & g.gmask) != g.gmask) continue;
+          const uint32_t m = (l0 & g.lmask) == g.lmask ? (uint32_t)tab.xoff[g.a] : 0u;
+          if (g.kind == SK_XF) {
+            sidx.x0 ^= m;
+          } else {
+#pragma unroll
+            for (int k = 0; k < NR; ++k)
+              if (g.b == k) sidx.xc[k] ^= m;
+          }
+        }
+        const R* q = p.pool + tab.qoff;
+        switch (prog) {
+#define SC_FAST_CASE(M)                                                                   \
+  case (M):                                                                               \
+    if constexpr (((M) >> NR) == 0)                                                       \
+      fast_stage<R, NR, (M), kTma>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last,   \
+                                   l0_last, p);                                           \
+    break;
+          SC_FAST_CASE(1) SC_FAST_CASE(2) SC_FAST_CASE(3) SC_FAST_CASE(4)
+          SC_FAST_CASE(5) SC_FAST_CASE(6) SC_FAST_CASE(7) SC_FAST_CASE(8)
+          SC_FAST_CASE(9) SC_FAST_CASE(10) SC_FAST_CASE(11) SC_FAST_CASE(12)
+          SC_FAST_CASE(13) SC_FAST_CASE(14) SC_FAST_CASE(15)
+#undef SC_FAST_CASE
+          case kProgNoRecord:
+            fast_stage<R, NR, 0, kTma>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last,
+                                       l0_last, p);
+            break;
+          default: break;
+        }
+        continue;
+      }
+      // the general record loop: one jump per record into code specialised on its
+      // register bits
+      A v[NV];
+#pragma unroll
+      for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
+      RegOff<NR> off;
 #pragma unroll
       for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
 
@@ -786,6 +885,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #define SC_G1ALLQ_CASE(M)                       \
   case (SK_G1ALLQ << 4) | (M):                  \
     if constexpr (((M) >> NR) == 0) {           \
+      if (g.b) prex<R, NR>(v, (uint32_t)g.b);   \
       g1allq<R, NR, (M)>(v, m);                 \
     }                                           \
     break;
@@ -806,32 +906,19 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
           default: break;
         }
       }
+      if (!last || kTma) __syncthreads();  // every read of `cur` in this stage is done
+      stage_exit<R, NR, kTma>(v, last, cur, wbase, tab, sidx, dst, gt_last, l0_last, p);
     }
     if constexpr (kTma) {
-      // stage the results in the linear layout and drain them with bulk stores
-      __syncthreads();  // every read of `cur` is done
-      {
-#pragma unroll
-        for (int j = 0; j < NV; ++j)
-          cur[l0_last | p.lastoff[j]] =
-              p.has_scale ? cmul(p.scale_re, p.scale_im, v[j]) : v[j];
-      }
+      // the last stage left the tile in the linear output layout: drain it with bulk
+      // stores
       fence_proxy_async_smem();
       __syncthreads();
       if (producer) {
-        A* dst = item_state(t) + base;
         for (uint32_t s = lane; s < nseg; s += nprod)
           bulk_store(dst + segoff[s], cur + s * seg_amps, seg_bytes);
         bulk_commit();
       }
-    } else {
-      A* __restrict__ dst = item_state(t) + base;
-      if (p.has_scale) {
-#pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = cmul(p.scale_re, p.scale_im, v[j]);
-      }
-#pragma unroll
-      for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
     }
   }
   if constexpr (kTma) {
@@ -994,8 +1081,8 @@ __global__ void __launch_bounds__(256, 2)
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
-          v[j] = bp[sw0 ^ tab.soff[j]];
-          w[j] = bl[sw0 ^ tab.soff[j]];
+          v[j] = bp[sw0 ^ tab.rd[j]];
+          w[j] = bl[sw0 ^ tab.rd[j]];
         }
       }
       psw0 = sw0;
@@ -1291,28 +1378,58 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
       p->tabs[s].xoff[b] =
           b < sw.nr ? (uint16_t)apply_swizzle(1u << st.R[b], zout, K) : (uint16_t)0;
     }
+    uint16_t off[16];
     for (int j = 0; j < 16; ++j) {
       uint32_t o = 0;
       if (j < nv)
         for (int b = 0; b < sw.nr; ++b)
           if (j & (1 << b)) o |= 1u << st.R[b];
-      p->tabs[s].off[j] = (uint16_t)o;
-      p->tabs[s].soff[j] = (uint16_t)apply_swizzle(o, zin[s], K);
+      off[j] = (uint16_t)o;
+    }
+    if (s == 0)
+      for (int j = 0; j < 16; ++j) p->off0[j] = off[j];
+    // the stage's code: one rotation record (plus slot folds) runs straight through
+    int n_rot = 0, n_other = 0, rot_g = -1;
+    for (int g = plan.stages[sw.s0 + s].g0; g < plan.stages[sw.s0 + s].g1; ++g) {
+      const SwGate& q = plan.gates[g];
+      if (q.kind == SK_XF || q.kind == SK_CXF) continue;
+      if (q.kind == SK_G1ALLQ && q.lmask == 0 && q.gmask == 0 && (q.a & 15) != 0 &&
+          ((q.a & 15) >> sw.nr) == 0) {
+        ++n_rot;
+        rot_g = g;
+      } else {
+        ++n_other;
+      }
+    }
+    SwStageTab& tb = p->tabs[s];
+    tb.prog = kProgGeneric;
+    tb.qoff = 0;
+    tb.xm = 0;
+    tb.pad = 0;
+    if (n_other == 0 && n_rot == 1) {
+      tb.prog = plan.gates[rot_g].a & 15;
+      tb.qoff = plan.gates[rot_g].moff - sw.pool0;
+      tb.xm = plan.gates[rot_g].b & (nv - 1);
+    } else if (n_other == 0 && n_rot == 0) {
+      tb.prog = kProgNoRecord;
+    }
+    for (int j = 0; j < 16; ++j) {
+      const int jx = j < nv ? j ^ tb.xm : j;
+      tb.rd[j] = s == 0 ? off[jx] : (uint16_t)apply_swizzle(off[jx], zin[s], K);
     }
     for (int j = 0; j < 16; ++j) {
       const int pj = (j < nv) ? st.perm[j] : j;
       if (pj < 0 || pj >= 16) return false;
-      p->tabs[s].wsoff[j] = (uint16_t)apply_swizzle(p->tabs[s].off[pj], zout, K);
+      tb.wsoff[j] = (uint16_t)apply_swizzle(off[pj], zout, K);
     }
+    if (s == ns - 1)
+      for (int j = 0; j < 16; ++j) p->lastoff[j] = off[(j < nv) ? st.perm[j] : j];
   }
   // slot folds act on the exchange slots: none may sit in the last stage
   for (int g = plan.stages[sw.s1 - 1].g0; g < plan.stages[sw.s1 - 1].g1; ++g)
     if (plan.gates[g].kind == SK_XF || plan.gates[g].kind == SK_CXF) return false;
-  const SwStage& last = p->stages[ns - 1];
   for (int j = 0; j < 16; ++j) {
-    const int pj = (j < nv) ? last.perm[j] : j;
-    p->gfirst[j] = host_spread(p->tabs[0].off[j], sw);
-    p->lastoff[j] = p->tabs[ns - 1].off[pj];
+    p->gfirst[j] = host_spread(p->off0[j], sw);
     p->glast[j] = host_spread_out(p->lastoff[j], sw);
   }
   // the sweep's record data: the pool entries appended while it was planned (records
@@ -1364,15 +1481,22 @@ bool check_exchanges_t(const Plan& plan, int64_t* st) {
       std::vector<int64_t> wslot((size_t)1 << T, -1), rslot((size_t)1 << T, -1);
       const SwStage& sw = p.stages[s - 1];
       const SwStage& sr = p.stages[s];
+      auto off_of = [&](const SwStage& g, int j) {
+        uint32_t o = 0;
+        for (int b = 0; b < nr; ++b)
+          if (j & (1 << b)) o |= 1u << g.R[b];
+        return o;
+      };
       for (int tid = 0; tid < threads; ++tid) {
         const uint32_t lw = l0_of(tid, sw, nr), lr = l0_of(tid, sr, nr);
         const uint32_t bw = slot_of(lw, p.tabs[s]), br = slot_of(lr, p.tabs[s]);
         for (int j = 0; j < NV; ++j) {
           const uint32_t a = bw ^ p.tabs[s - 1].wsoff[j];  // register j leaves as perm[j]
-          const uint32_t b = br ^ p.tabs[s].soff[j];
+          const uint32_t b = br ^ p.tabs[s].rd[j];
           if (a >= (1u << T) || b >= (1u << T) || wslot[a] >= 0 || rslot[b] >= 0) return false;
-          wslot[a] = lw | p.tabs[s - 1].off[sw.perm[j]];
-          rslot[b] = lr | p.tabs[s].off[j];
+          wslot[a] = lw | off_of(sw, sw.perm[j]);
+          // register j takes the amplitude of register j ^ xm (the folded leading X)
+          rslot[b] = lr | off_of(sr, j ^ p.tabs[s].xm);
         }
         for (int a = 0; a < nr; ++a)
           if (p.tabs[s - 1].xoff[a] != slot_of(1u << sw.R[a], p.tabs[s])) return false;
@@ -1389,7 +1513,7 @@ bool check_exchanges_t(const Plan& plan, int64_t* st) {
             for (int t = t0; t < t0 + group; ++t, ++n) {
               const uint32_t a = side == 0
                   ? slot_of(l0_of(t, sw, nr), p.tabs[s]) ^ p.tabs[s - 1].wsoff[j]
-                  : slot_of(l0_of(t, sr, nr), p.tabs[s]) ^ p.tabs[s].soff[j];
+                  : slot_of(l0_of(t, sr, nr), p.tabs[s]) ^ p.tabs[s].rd[j];
               seen |= 1u << (a & ((1u << K) - 1u));
             }
             ++st[2];

@@ -884,13 +884,16 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       // runs of uncontrolled 2x2 gates on distinct register bits become one record
       std::vector<std::pair<int, const double*>> run;
       std::vector<int64_t> run_ops;
-      // rotation-form record for the gates of `part` (increasing register bit)
-      auto emit_rotation = [&](const std::vector<int>& part, const std::vector<double>& qs) {
+      // rotation-form record for the gates of `part` (increasing register bit); the
+      // gates of `xpart` are U X in rotation form, so the record starts with X on them
+      auto emit_rotation = [&](const std::vector<int>& part, const std::vector<double>& qs,
+                               const std::vector<int>& xpart) {
         SwGate sg;
         std::memset(&sg, 0, sizeof sg);
         sg.moff = (int32_t)plan.pool.size();
         sg.kind = SK_G1ALLQ;
         for (int i : part) sg.a |= 1 << run[i].first;
+        for (int i : xpart) sg.b |= 1 << run[i].first;
         // t per gate, then the input- and output-phase tables over the subsets s of
         // the record's gates (bit k of s: gate k, in increasing register bit)
         const int K = (int)part.size();
@@ -937,18 +940,28 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         std::vector<int> order(run.size());
         for (size_t i = 0; i < run.size(); ++i) order[i] = (int)i;
         std::sort(order.begin(), order.end(), [&](int x, int y) { return run[x].first < run[y].first; });
-        std::vector<int> rot, mat;
+        std::vector<int> rot, mat, xrot;
         std::vector<double> qs;
         double sr = sw.scale_re, si = sw.scale_im;
         for (int i : order) {
           double q[5], fr, fi;
           bool ok = rotation_form(run[i].second, pp.rot_min_c, q, &fr, &fi);
+          bool lead_x = false;
+          if (!ok) {
+            // |u00| small: U = (U X) X, and U X (the columns of U swapped) has
+            // |(U X)00| = |u01| close to 1, so it takes the rotation form after an X
+            const double* u = run[i].second;
+            const double ux[8] = {u[2], u[3], u[0], u[1], u[6], u[7], u[4], u[5]};
+            ok = rotation_form(ux, pp.rot_min_c, q, &fr, &fi);
+            lead_x = ok;
+          }
           const double nr = sr * fr - si * fi, ni = sr * fi + si * fr;
           // the stored amplitudes grow by 1 / |scalar| within the sweep: keep the
           // matrix form once the sweep's own scalar would drop below the floor
           if (ok && std::hypot(nr, ni) < pp.scale_floor) ok = false;
           if (ok) {
             rot.push_back(i);
+            if (lead_x) xrot.push_back(i);
             qs.insert(qs.end(), q, q + 5);
             sr = nr;
             si = ni;
@@ -957,7 +970,7 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
           }
         }
         if (!rot.empty()) {
-          emit_rotation(rot, qs);
+          emit_rotation(rot, qs, xrot);
           sw.scale_re = sr;
           sw.scale_im = si;
         }

@@ -244,6 +244,10 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
                 for (int k = 0; k < K; ++k) sub |= ((j >> bits[k]) & 1) << k;
                 return sub;
               };
+              for (int bit = 0; bit < NR; ++bit)  // the record's leading X
+                if ((g.b >> bit) & 1)
+                  for (int j = 0; j < NV; ++j)
+                    if (!(j & (1 << bit))) std::swap(v[j], v[j | (1 << bit)]);
               for (int j = 0; j < NV; ++j)
                 if (const int sub = subset(j)) v[j] = cm(lam[2 * (sub - 1)], lam[2 * (sub - 1) + 1], v[j]);
               for (int k = 0; k < K; ++k) {

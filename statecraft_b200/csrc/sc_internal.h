@@ -76,7 +76,9 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        the products of their e^{i lam} and of their e^{i phi} over every non-empty
 //        subset of the gates (2 x (2^K - 1) complex; bit k of the subset index is the
 //        k-th gate in increasing register bit).  The scalars s_g are carried in
-//        SwSweep::scale and applied to every amplitude at a sweep's store.
+//        SwSweep::scale and applied to every amplitude at a sweep's store.  b: register
+//        bits whose gate is U X in rotation form (|u00| too small for U itself): the
+//        record first applies X on those bits.
 // SK_XF / SK_CXF: X on register bit a (controlled by register bit b for CXF) whose
 //        other controls lie outside the registers (lmask: tile positions, gmask:
 //        global qubits), last to touch its bits in a stage that is not the sweep's

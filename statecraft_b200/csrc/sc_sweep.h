@@ -12,22 +12,36 @@ constexpr int kSweepMaxStages = 80;
 constexpr int kSweepMaxGates = 78;   // stages <= gates + 2
 constexpr int kSweepMaxPool = 2048;  // matrix reals
 
-// Per-stage register tables computed on the host: off[j] is the tile offset of
-// register j (the OR of 1 << R[k] over the set bits k of j), soff[j] its slot in
-// the shared-memory layout the stage reads, wsoff[j] the slot register j is written
-// to when the stage ends (register perm[j] in the next stage's layout) and xoff[a]
-// the offset of register bit a in that layout (slot folds).  Each exchange between
-// two stages has its own XOR swizzle, slot(i) = i ^ sum_k parity(i & rows[k]) << k
-// over the low K slot bits (K = log2 of the amplitudes per 128-byte row); rows[]
-// only read bits >= K, so every swizzle is a bijection and XOR-linear over disjoint
-// bits.  rows[] here is the swizzle of the layout this stage reads; bit 15 of
-// rows[0] marks one that differs from the fixed default (rows[k] = 1 << (K + k)).
+// Per-stage register tables computed on the host.  off[j] below is the tile offset
+// of register j (the OR of 1 << R[k] over the set bits k of j); rd[j] is the slot
+// register j is read from, relative to the stage's read base (the thread's l0 in
+// the linear layout for stage 0, its swizzled l0 otherwise): the slot of tile
+// offset off[j ^ xm], xm being an X on register bits that the stage's rotation
+// record starts with and that is folded into the read (0 elsewhere).  wsoff[j] is
+// the slot register j is written to when the stage ends (register perm[j] in the
+// next stage's layout) and xoff[a] the offset of register bit a in that layout
+// (slot folds).  Each exchange between two stages has its own XOR swizzle,
+// slot(i) = i ^ sum_k parity(i & rows[k]) << k over the low K slot bits (K = log2
+// of the amplitudes per 128-byte row); rows[] only read bits >= K, so every
+// swizzle is a bijection and XOR-linear over disjoint bits.  rows[] here is the
+// swizzle of the layout this stage reads; bit 15 of rows[0] marks one that differs
+// from the fixed default (rows[k] = 1 << (K + k)).
+// prog selects the stage's code: 0 = the general record loop; 1..15 = a stage whose
+// only register record is one rotation-form record on register-bit mask prog (pool
+// offset qoff), any other records being slot folds; 16 = a stage with slot folds
+// only.  Such a stage runs as straight-line code from its shared-memory read to its
+// exit store.
+constexpr int kProgGeneric = 0;
+constexpr int kProgNoRecord = 16;
 struct SwStageTab {
-  uint16_t off[16];
-  uint16_t soff[16];
+  uint16_t rd[16];
   uint16_t wsoff[16];
   uint16_t xoff[4];
   uint16_t rows[4];
+  int32_t prog;
+  int32_t qoff;
+  int32_t xm;
+  int32_t pad;
 };
 
 template <typename R>
@@ -47,6 +61,7 @@ struct SweepParams {
   int32_t hq[SW_MAX_HIGH];  // physical bit of tile position L + k (input layout)
   int32_t hs[SW_MAX_HIGH];  // the same bits ascending (tile enumeration)
   uint8_t outp[32];         // physical bit of tile position p in the output layout
+  uint16_t off0[16];     // tile offset of register j in the first stage (linear layout)
   uint32_t gfirst[16];   // global offset of register j in the first stage's layout
   uint32_t glast[16];    // global offset register j is stored to (last stage, perm applied)
   uint16_t lastoff[16];  // tile offset register j is stored to (last stage, perm applied)

@@ -206,7 +206,8 @@ def test_rotation_form_scalar_stays_in_range():
 
 def test_runs_mixing_rotation_and_matrix_gates():
     # layers of u3 gates where some have |u00| below the rotation-form bound (0.05):
-    # a run of commuting gates splits into a rotation-form record and a matrix record
+    # those take the rotation form as U X, so their record starts with an X on their
+    # bits (folded into the stage's read where the record is the stage's only one)
     from statecraft_b200 import quantum as Q
 
     n = 12

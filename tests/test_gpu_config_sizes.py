@@ -4,9 +4,15 @@
   with 29 controls + RZZ on a seeded pair, angle seed 3030) for two layers, fused
   plan on the GPU; the full 2^30-amplitude state within 1e-12 max-abs of the
   oracle and countsAll(8192) with seed 42 identical, except draws that fall within
-  1e-12 of a CDF boundary (the two prefix sums round differently there), which are
-  counted and must be rare.  Reference rules: StatevectorEngineTest.java:393-406
-  (1e-12), StatevectorEngine.java:229-338 (measurement).
+  the rounding band of a CDF boundary, which are counted and must be rare.  The
+  reference's CDF is a left-to-right running sum (StatevectorEngine.java:314-323);
+  the GPU's is a chunk sum, a scan of the chunk sums and a running sum inside the
+  chunk.  The recursive-summation bound (Higham, Accuracy and Stability of Numerical
+  Algorithms, 2nd ed., eq. 4.4) limits each to (terms summed) * 2^-53 * value, so at
+  entry j of a 2^30-entry CDF the two can differ by up to (j + 2^11 + 2^19) * 2^-53
+  * cdf[j]; a draw closer than that to an entry can land on either side.  Reference
+  rules: StatevectorEngineTest.java:393-406 (1e-12), StatevectorEngine.java:229-338
+  (measurement).
 - 26 qubits, complex128: the hardware-efficient ansatz of the adjoint workload
   (12 layers of RY, RZ and a CNOT ring, 624 angles, 64 random Pauli terms); <H>
   against the oracle, and the fused adjoint gradient on 8 angles against exact
@@ -97,8 +103,14 @@ def test_c2_30q_two_layers_state_and_counts_match_oracle():
     mism = np.nonzero(gpu_out != want_out)[0]
     for k in mism:
         j = int(want_out[k])
-        edges = [cdf[j - 1] if j > 0 else 0.0, cdf[j]]
-        assert min(abs(u[k] - e) for e in edges) < 1e-12, (k, gpu_out[k], want_out[k])
+        for e in (j - 1, j):  # the entries on either side of the reference's outcome
+            band = (e + 1 + (1 << 11) + (1 << 19)) * 2.0 ** -53 * (cdf[e] if e >= 0 else 0.0)
+            if e >= 0 and abs(u[k] - cdf[e]) <= band:
+                break
+        else:
+            raise AssertionError((k, int(gpu_out[k]), j, float(u[k])))
+        print("30q counts: shot %d drew %.17g, %.3e from a CDF entry (GPU %d, oracle %d)"
+              % (k, u[k], min(abs(u[k] - cdf[j]), abs(u[k] - cdf[j - 1])), gpu_out[k], j))
     assert len(mism) <= 2
 
 
