@@ -256,6 +256,14 @@ SC_API int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_op
  * conflict}.  Returns the number of sweeps, or SC_ESTATE if a table is inconsistent. */
 SC_API int32_t sc_debug_check_exchanges(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
                                  int32_t low_qubits, int32_t nr, int32_t dtype, int64_t* stats);
+/* Checks the whole-tile tensor copies (TMA boxes) the sweep kernel would use for the
+ * plan of ops over `batch` states: for each sweep whose tile is a box of the state
+ * tensor, every tile position of a spread of tiles is copied from the amplitude the
+ * sweep's tile enumeration assigns to it.  stats[2] = {sweeps with a box form, tiles
+ * checked}.  Returns the number of sweeps, or SC_ESTATE on a mismatch. */
+SC_API int32_t sc_debug_check_tile_tensors(int32_t n, const sc_op* ops, int64_t n_ops,
+                                           int32_t tile_qubits, int32_t low_qubits, int32_t nr,
+                                           int32_t dtype, int64_t batch, int64_t* stats);
 /* As sc_debug_emulate_sweeps for one trajectory of a batch: Pauli slot j sits after
  * op slot_after[j] (non-decreasing) on qubit slot_qubit[j] and applies paulis[j]
  * (0 = I, 1 = X, 2 = Y, 3 = Z), planned the way sc_trajectories plans slots. */

@@ -151,6 +151,10 @@ SIGNATURES = {
     "sc_debug_check_exchanges": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                                   ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                   ctypes.c_int32, _P(ctypes.c_int64)]),
+    "sc_debug_check_tile_tensors": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
+                                                     ctypes.c_int32, ctypes.c_int32,
+                                                     ctypes.c_int32, ctypes.c_int32,
+                                                     ctypes.c_int64, _P(ctypes.c_int64)]),
     "sc_debug_emulate_slots": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                                 ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                                 ctypes.c_double, _P(ctypes.c_int64),

@@ -22,7 +22,10 @@
 // Every mbarrier wait is bounded (about a second of clock cycles); on timeout the
 // CTA records an error in `err`, waits (bounded) for the copies it issued and
 // returns, and the host reports SC_ETIMEOUT.
+#include <cuda.h>
+
 #include <algorithm>
+#include <cstdlib>
 #include <memory>
 #include <mutex>
 #include <type_traits>
@@ -483,6 +486,16 @@ __device__ __forceinline__ void prex(typename Amp<R>::type (&v)[1 << NR], uint32
   SC_CASE_2(K, 1, 2, F) SC_CASE_2(K, 1, 3, F) SC_CASE_2(K, 2, 0, F) SC_CASE_2(K, 2, 1, F) \
   SC_CASE_2(K, 2, 3, F) SC_CASE_2(K, 3, 0, F) SC_CASE_2(K, 3, 1, F) SC_CASE_2(K, 3, 2, F)
 
+// tile position bits -> physical offset in the input layout (host, sweep parameters)
+template <typename P>
+uint64_t host_spread_t(uint64_t x, const P& p) {
+  uint64_t g = x & ((1ULL << p.L) - 1ULL);
+  uint64_t hi = x >> p.L;
+  for (int k = 0; hi; ++k, hi >>= 1)
+    if (hi & 1ULL) g |= 1ULL << p.hq[k];
+  return g;
+}
+
 // local tile index -> global offset (n <= 32: 32-bit)
 template <typename P>
 __device__ __forceinline__ uint32_t spread32(uint32_t x, const P& p) {
@@ -515,7 +528,7 @@ __device__ __forceinline__ uint32_t spread_out32(uint32_t x, const P& p) {
 
 // physical offset of tile t: its index bits spread over the non-tile bits
 template <typename P>
-__device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
+__host__ __device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
   uint32_t base = t << p.L;
 #pragma unroll 1
   for (int k = 0; k < p.h; ++k) base = insert_zero32(base, p.hs[k]);
@@ -601,17 +614,19 @@ constexpr int sweep_max_regs() {
 
 constexpr long long kWaitLimitCycles = 2000000000LL;  // ~1 s at 2 GHz
 
+// two tile buffers, the mbarriers and abort flag of the bulk-copy pipeline (64
+// bytes), and the Pauli choices of a batched sweep's slots (128 bytes)
 template <typename R>
-__host__ __device__ constexpr size_t sweep_smem_bytes(int T, int h, bool tma, int stages) {
-  (void)stages;
-  return tma ? 2 * (sizeof(typename Amp<R>::type) << T) + 64 + 4 * ((size_t)1 << h)
-             : 2 * (sizeof(typename Amp<R>::type) << T);
+__host__ __device__ constexpr size_t sweep_smem_bytes(int T) {
+  return 2 * (sizeof(typename Amp<R>::type) << T) + 64 + 128;
 }
 
-// kTma = true: double-buffered bulk-copy pipeline (worth it for long segments);
-// kTma = false: direct 128-/64-bit loads and stores, one exchange buffer.
-// kBatch = true (direct path only): the sweep runs over p.batch states back to
-// back, and Pauli slots read the trajectory's choices, staged in shared memory.
+// kTma = true: each tile is one bulk tensor copy (TMA) into a double-buffered tile
+// buffer and leaves as one bulk tensor store; kTma = false: per-thread cp.async
+// copies of each thread's first-stage registers and direct 128-/64-bit stores
+// (sweeps whose tile is not a box of the state tensor, e.g. a layout change).
+// kBatch = true: the sweep runs over p.batch states back to back, and Pauli slots
+// read the trajectory's choices, staged in shared memory.
 template <typename R, int NR, bool kTma, bool kBatch>
 __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep_max_regs<R, NR>()))
     k_sweep(typename Amp<R>::type* __restrict__ st, const __grid_constant__ SweepParams<R> p,
@@ -624,17 +639,10 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   A* const buf1 = buf0 + tile_amps;
   uint64_t* const bars = reinterpret_cast<uint64_t*>(buf1 + tile_amps);
   int* const s_abort = reinterpret_cast<int*>(bars + 2);
-  uint32_t* const segoff = reinterpret_cast<uint32_t*>(bars + 8);
+  // Pauli choices of the current trajectory for this sweep's slots
+  uint8_t* const codes = reinterpret_cast<uint8_t*>(bars + 8);
   const uint32_t tid = threadIdx.x;
-  const uint32_t lane = tid & 31u;
-  // warp 0 (all of it, or the whole block when it is smaller) issues every bulk copy
-  const uint32_t nprod = blockDim.x < 32u ? blockDim.x : 32u;
-  const unsigned pmask = nprod == 32u ? 0xffffffffu : ((1u << nprod) - 1u);
-  const bool producer = tid < nprod;
   const int ns = p.n_stages;
-  const uint32_t nseg = 1u << p.h;
-  const uint32_t seg_amps = 1u << p.L;
-  const uint32_t seg_bytes = seg_amps * (uint32_t)sizeof(A);
   const uint32_t tile_bytes = tile_amps * (uint32_t)sizeof(A);
   // work items: (state, tile) pairs, tile-major within a state; one state unless
   // the sweep runs over a batch of trajectories
@@ -644,18 +652,9 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
     if constexpr (kBatch) return st + ((uint64_t)(it >> p.tiles_log2) << p.nq);
     return st;
   };
-  // Pauli choices of the current trajectory for this sweep's slots
-  uint8_t* const codes = reinterpret_cast<uint8_t*>(buf1 + tile_amps);
   uint32_t codes_for = 0xffffffffu;
 
   if constexpr (kTma) {
-    // global offset of each segment (the high tile bits spread onto hq)
-    for (uint32_t sidx = tid; sidx < nseg; sidx += blockDim.x) {
-      uint32_t g = 0;
-      for (int k = 0; k < p.h; ++k)
-        if ((sidx >> k) & 1u) g |= 1u << p.hq[k];
-      segoff[sidx] = g;
-    }
     if (tid == 0) {
       mbar_init(&bars[0], 1);
       mbar_init(&bars[1], 1);
@@ -664,14 +663,18 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
     }
     __syncthreads();
   }
-
-  auto issue_load = [&](uint32_t t, int b) {
-    const A* src = item_state(t) + tile_base(t & tile_mask, p);
-    A* dst = b ? buf1 : buf0;
-    if (lane == 0) mbar_arrive_expect_tx(&bars[b], tile_bytes);
-    __syncwarp(pmask);
-    for (uint32_t s = lane; s < nseg; s += nprod)
-      bulk_load(dst + s * seg_amps, src + segoff[s], seg_bytes, &bars[b]);
+  // box coordinates of work item `it` in the state tensor
+  auto item_coords = [&](uint32_t it, int32_t* c) {
+#pragma unroll
+    for (int k = 0; k < kTileTensorMaxRank; ++k)
+      c[k] = (int32_t)((it >> p.tm_shift[k]) & p.tm_mask[k]);
+  };
+  // thread 0 issues the whole tile as one tensor copy
+  auto issue_load = [&](uint32_t it, int b) {
+    int32_t c[kTileTensorMaxRank];
+    item_coords(it, c);
+    mbar_arrive_expect_tx(&bars[b], tile_bytes);
+    tensor_load(b ? buf1 : buf0, p.tmap, c, p.tm_rank, &bars[b]);
   };
 
   // first (load) and last (store) register layouts are tile-invariant
@@ -692,7 +695,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   uint32_t t = blockIdx.x;
   uint32_t i = 0;
   if constexpr (kTma) {
-    if (producer && t < tiles) issue_load(t, 0);
+    if (tid == 0 && t < tiles) issue_load(t, 0);
   } else {
     if (t < tiles) prefetch_own(t, buf0);
     cp_async_commit();
@@ -710,9 +713,10 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
     }
     if constexpr (kTma) {
       const uint32_t tn = t + gridDim.x;
-      if (producer && tn < tiles) {
-        bulk_wait_read_all();  // the other buffer's previous bulk stores have read it
-        fence_proxy_async_smem();
+      if (tid == 0 && tn < tiles) {
+        // the other buffer: its last tile's bulk store has finished reading it (every
+        // thread's reads of it ended before that tile's closing barrier)
+        bulk_wait_read_all();
         issue_load(tn, b ^ 1);
       }
       if (!mbar_wait_bounded(&bars[b], (i >> 1) & 1u, kWaitLimitCycles)) {
@@ -910,25 +914,26 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       stage_exit<R, NR, kTma>(v, last, cur, wbase, tab, sidx, dst, gt_last, l0_last, p);
     }
     if constexpr (kTma) {
-      // the last stage left the tile in the linear output layout: drain it with bulk
-      // stores
+      // the last stage left the tile in the linear output layout: one bulk tensor
+      // store writes it back
       fence_proxy_async_smem();
       __syncthreads();
-      if (producer) {
-        for (uint32_t s = lane; s < nseg; s += nprod)
-          bulk_store(dst + segoff[s], cur + s * seg_amps, seg_bytes);
+      if (tid == 0) {
+        int32_t c[kTileTensorMaxRank];
+        item_coords(t, c);
+        tensor_store(p.tmap, c, p.tm_rank, cur);
         bulk_commit();
       }
     }
   }
   if constexpr (kTma) {
-    if (aborted && producer) {
+    if (aborted && tid == 0) {
       // wait (bounded) for the loads this CTA still has in flight before leaving
       const uint32_t tn = t + gridDim.x;
       mbar_wait_bounded(&bars[i & 1u], (i >> 1) & 1u, kWaitLimitCycles);
       if (tn < tiles) mbar_wait_bounded(&bars[(i + 1) & 1u], ((i + 1) >> 1) & 1u, kWaitLimitCycles);
     }
-    if (producer) bulk_wait_all();
+    if (tid == 0) bulk_wait_all();
   }
 }
 
@@ -1149,8 +1154,166 @@ struct LaunchCache {
 };
 LaunchCache g_cache;
 
-// Bulk copies pay off once a segment is long; shorter segments use direct loads.
-constexpr uint32_t kTmaMinSegmentBytes = 2048;
+// cuTensorMapEncodeTiled, looked up once through the runtime (no link-time
+// dependency on the driver library)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+  static std::once_flag once;
+  static EncodeTiledFn fn = nullptr;
+  std::call_once(once, [] {
+    if (const char* v = getenv("STATECRAFT_B200_TMA"))
+      if (atoi(v) == 0) return;  // tensor copies off: every sweep takes the cp.async path
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(f);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// The state (or the batch of states) as the copy engine sees it, so that each tile
+// of a sweep is one box (layout in sc_sweep.h): dims, byte strides and box of each
+// dim, innermost first, with the coordinate rules stored into p.  False when the
+// tile is not a box of at most kTileTensorMaxRank dims in its linear order.
+struct TileTensor {
+  int rank = 0;
+  uint64_t dims[kTileTensorMaxRank];     // in 8-byte elements for dim 0, else in steps
+  uint64_t strides[kTileTensorMaxRank];  // bytes per step (dim 0: the element)
+  uint32_t box[kTileTensorMaxRank];
+};
+
+template <typename R>
+bool tile_tensor_geometry(SweepParams<R>& p, TileTensor* tt) {
+  using A = typename Amp<R>::type;
+  p.tm_rank = 0;
+  for (int k = 0; k < kTileTensorMaxRank; ++k) {
+    p.tm_shift[k] = 0;
+    p.tm_mask[k] = 0;
+  }
+  if (p.relayout || p.L < 1) return false;
+  const int n = p.nq;
+  // tile bits: 0..L-1 and hq[] ascending, so the box lands in the linear tile order
+  uint64_t tile = (1ULL << p.L) - 1ULL;
+  for (int k = 0; k < p.h; ++k) {
+    if (p.hq[k] < p.L || p.hq[k] >= n || (k > 0 && p.hq[k] <= p.hq[k - 1])) return false;
+    tile |= 1ULL << p.hq[k];
+  }
+  const int e = (int)(sizeof(A) / 8);  // 8-byte elements per amplitude
+  int rank = 0, nontile_below = 0;
+  for (int b = 0; b < n;) {
+    const bool in = ((tile >> b) & 1ULL) != 0;
+    int len = 0;
+    while (b + len < n && (((tile >> (b + len)) & 1ULL) != 0) == in) ++len;
+    // a box dim holds at most 256 elements: long tile runs take several dims
+    for (int start = b, rem = len; rem > 0;) {
+      const int cap = in ? (start == 0 ? (e == 2 ? 7 : 8) : 8) : 32;
+      const int w = std::min(rem, cap);
+      if (rank >= kTileTensorMaxRank) return false;
+      tt->dims[rank] = (uint64_t)(start == 0 ? e : 1) << w;
+      tt->box[rank] = in ? (uint32_t)tt->dims[rank] : 1u;
+      tt->strides[rank] = start == 0 ? 8u : (uint64_t)sizeof(A) << start;
+      p.tm_shift[rank] = in ? 0 : nontile_below;
+      p.tm_mask[rank] = in ? 0u : (uint32_t)((1ULL << w) - 1ULL);
+      if (!in) nontile_below += w;
+      ++rank;
+      start += w;
+      rem -= w;
+    }
+    b += len;
+  }
+  if (p.batch > 1) {  // the state index of a batch
+    if (rank >= kTileTensorMaxRank) return false;
+    tt->dims[rank] = (uint64_t)p.batch;
+    tt->box[rank] = 1u;
+    tt->strides[rank] = (uint64_t)sizeof(A) << n;
+    p.tm_shift[rank] = p.tiles_log2;
+    p.tm_mask[rank] = 0xffffffffu;
+    ++rank;
+  }
+  tt->rank = rank;
+  return true;
+}
+
+// Fills p.tmap for the state at `state` and sets p.tm_rank; false (tm_rank = 0) when
+// the sweep has no box form or the encoder is unavailable or refuses it.
+template <typename R>
+bool make_tile_tensor(void* state, SweepParams<R>& p) {
+  TileTensor tt;
+  EncodeTiledFn encode = encode_tiled_fn();
+  if (!encode || !tile_tensor_geometry(p, &tt)) {
+    p.tm_rank = 0;
+    return false;
+  }
+  cuuint64_t dims[kTileTensorMaxRank], strides[kTileTensorMaxRank];
+  cuuint32_t box[kTileTensorMaxRank], estr[kTileTensorMaxRank];
+  for (int k = 0; k < tt.rank; ++k) {
+    dims[k] = tt.dims[k];
+    strides[k] = tt.strides[k];
+    box[k] = tt.box[k];
+    estr[k] = 1;
+  }
+  static_assert(sizeof(p.tmap) == sizeof(CUtensorMap), "tensor map storage");
+  const CUresult r = encode(reinterpret_cast<CUtensorMap*>(p.tmap), CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                            (cuuint32_t)tt.rank, state, dims, strides + 1, box, estr,
+                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    p.tm_rank = 0;
+    return false;
+  }
+  p.tm_rank = tt.rank;
+  return true;
+}
+
+// Host check of the box geometry: for every work item and every tile position, the
+// global amplitude the box copies to that position of the tile buffer (copy-engine
+// addressing: shared offset = box-linear index, global offset = sum over dims of
+// (coordinate + index) * stride) is the one the sweep's tile enumeration assigns
+// to it.  stats[0] += sweeps with a box form, stats[1] += work items checked.
+template <typename R>
+bool check_tile_tensor(SweepParams<R>& p, int64_t* stats) {
+  using A = typename Amp<R>::type;
+  TileTensor tt;
+  if (!tile_tensor_geometry(p, &tt)) return true;  // cp.async path: nothing to check
+  const int e = (int)(sizeof(A) / 8);
+  uint64_t box_elems = 1;
+  for (int k = 0; k < tt.rank; ++k) box_elems *= tt.box[k];
+  if (box_elems != (uint64_t)e << p.T) return false;  // the tile is exactly one box
+  if (tt.dims[0] != tt.box[0] || (tt.box[0] * 8u) % 16u != 0) return false;
+  const uint64_t items = (uint64_t)p.tiles * (uint64_t)p.batch;
+  const uint64_t step = items > 4096 ? items / 4096 : 1;  // a spread of items
+  for (uint64_t it = 0; it < items; it += step) {
+    int32_t c[kTileTensorMaxRank];
+    for (int k = 0; k < tt.rank; ++k) {
+      c[k] = (int32_t)((it >> p.tm_shift[k]) & p.tm_mask[k]);
+      if ((uint64_t)c[k] + tt.box[k] > tt.dims[k]) return false;
+    }
+    const uint64_t tile = it & ((uint64_t)p.tiles - 1ULL);
+    const uint64_t st = it >> p.tiles_log2;
+    const uint64_t base = tile_base((uint32_t)tile, p);
+    for (uint64_t sm = 0; sm < box_elems; sm += (uint64_t)e) {
+      // decompose the shared offset into per-dim box indices, dim 0 fastest
+      uint64_t rest = sm, byte = 0;
+      for (int k = 0; k < tt.rank; ++k) {
+        const uint64_t idx = rest % tt.box[k];
+        rest /= tt.box[k];
+        byte += ((uint64_t)c[k] + idx) * tt.strides[k];
+      }
+      const uint64_t want = (st << p.nq) | base | host_spread_t(sm / (uint64_t)e, p);
+      if (byte != want * sizeof(A)) return false;
+    }
+    ++stats[1];
+  }
+  ++stats[0];
+  return true;
+}
 
 template <typename R, int NR, bool kTma, bool kBatch>
 cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_count,
@@ -1169,9 +1332,7 @@ cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_cou
   }
   const int threads = 1 << (p.T - NR);
   if (threads > sweep_max_threads<R, NR>()) return cudaErrorInvalidConfiguration;
-  // bulk copies move whole 16-byte multiples from 16-byte aligned addresses
-  if (kTma && ((sizeof(A) << p.L) & 15u) != 0) return cudaErrorInvalidConfiguration;
-  const size_t smem = sweep_smem_bytes<R>(p.T, p.h, kTma, p.n_stages) + (kBatch ? 128 : 0);
+  const size_t smem = sweep_smem_bytes<R>(p.T);
   if (smem > 200 * 1024) return cudaErrorInvalidConfiguration;
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
@@ -1183,19 +1344,17 @@ cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_cou
 }
 
 template <typename R, int NR>
-cudaError_t launch_pick(void* state, const SweepParams<R>& p, int* err, int sm_count,
-                        cudaStream_t s) {
-  const uint32_t seg_bytes = (uint32_t)sizeof(typename Amp<R>::type) << p.L;
-  if (p.batch > 1 || p.n_local_slots > 0) return launch_nr<R, NR, false, true>(state, p, err, sm_count, s);
-  // the bulk-copy store writes segments back where they came from: no relayout
-  if (seg_bytes >= kTmaMinSegmentBytes && !p.relayout)
-    return launch_nr<R, NR, true, false>(state, p, err, sm_count, s);
-  return launch_nr<R, NR, false, false>(state, p, err, sm_count, s);
+cudaError_t launch_pick(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
+  const bool batch = p.batch > 1 || p.n_local_slots > 0;
+  if (make_tile_tensor<R>(state, p))
+    return batch ? launch_nr<R, NR, true, true>(state, p, err, sm_count, s)
+                 : launch_nr<R, NR, true, false>(state, p, err, sm_count, s);
+  return batch ? launch_nr<R, NR, false, true>(state, p, err, sm_count, s)
+               : launch_nr<R, NR, false, false>(state, p, err, sm_count, s);
 }
 
 template <typename R>
-cudaError_t launch_t(void* state, const SweepParams<R>& p, int* err, int sm_count,
-                     cudaStream_t s) {
+cudaError_t launch_t(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
   switch (p.nr) {
     case 1: return launch_pick<R, 1>(state, p, err, sm_count, s);
     case 2: return launch_pick<R, 2>(state, p, err, sm_count, s);
@@ -1326,6 +1485,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
   if (ns < 1 || ns > kSweepMaxStages || sw.nr > SW_MAX_NR) return false;
   const int g_lo = plan.stages[sw.s0].g0, g_hi = plan.stages[sw.s1 - 1].g1;
   if (g_hi - g_lo > kSweepMaxGates) return false;
+  p->tm_rank = 0;
   p->T = sw.T;
   p->L = sw.L;
   p->h = sw.h;
@@ -1525,6 +1685,27 @@ bool check_exchanges_t(const Plan& plan, int64_t* st) {
 }
 
 }  // namespace
+
+namespace {
+
+template <typename R>
+bool check_tile_tensors_t(const Plan& plan, int64_t batch, int64_t* stats) {
+  std::unique_ptr<SweepParams<R>> pp(new SweepParams<R>());
+  for (size_t k = 0; k < plan.sweeps.size(); ++k) {
+    if (!fill_params(plan, k, pp.get())) return false;
+    pp->batch = batch;
+    if (!check_tile_tensor(*pp, stats)) return false;
+  }
+  return true;
+}
+
+}  // namespace
+
+bool check_tile_tensors(const Plan& plan, int dtype, int64_t batch, int64_t* stats) {
+  stats[0] = stats[1] = 0;
+  return dtype == SC_C64 ? check_tile_tensors_t<float>(plan, batch, stats)
+                         : check_tile_tensors_t<double>(plan, batch, stats);
+}
 
 bool check_exchange_tables(const Plan& plan, int dtype, int64_t* stats) {
   for (int i = 0; i < 4; ++i) stats[i] = 0;

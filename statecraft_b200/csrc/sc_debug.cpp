@@ -426,4 +426,21 @@ int32_t sc_debug_check_exchanges(int32_t n, const sc_op* ops, int64_t n_ops, int
   return (int32_t)plan.sweeps.size();
 }
 
+int32_t sc_debug_check_tile_tensors(int32_t n, const sc_op* ops, int64_t n_ops,
+                                    int32_t tile_qubits, int32_t low_qubits, int32_t nr,
+                                    int32_t dtype, int64_t batch, int64_t* stats) {
+  std::vector<PGate> gates;
+  int rc = normalise_all(n, ops, n_ops, gates);
+  if (rc != SC_OK) return rc;
+  if (!stats) return fail(SC_EINVAL, "stats is null");
+  if (dtype != SC_C64 && dtype != SC_C128) return fail(SC_EINVAL, "dtype must be SC_C64 or SC_C128");
+  if (batch < 1) return fail(SC_EINVAL, "batch must be positive");
+  PlanParams pp = debug_params(tile_qubits, low_qubits, nr, -1.0);
+  Plan plan = plan_sweeps(gates, n, pp);
+  if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+  if (!check_tile_tensors(plan, dtype, batch, stats))
+    return fail(SC_ESTATE, "a tile tensor copy does not match the sweep's tile enumeration");
+  return (int32_t)plan.sweeps.size();
+}
+
 }  // extern "C"

@@ -122,6 +122,91 @@ __device__ __forceinline__ void bulk_load(void* dst_smem, const void* src, uint3
       : "memory");
 }
 
+// Tiled bulk tensor copy (TMA) of one box, global -> shared, completing on an
+// mbarrier.  tmap: generic address of a CUtensorMap in kernel-parameter or global
+// memory; c[0..rank-1]: box coordinates (innermost first; c[0] must keep the copy
+// 16-byte aligned).  No cluster multicast.
+__device__ __forceinline__ void tensor_load(void* dst_smem, const void* tmap, const int32_t* c,
+                                            int rank, uint64_t* bar) {
+  const uint64_t m = reinterpret_cast<uint64_t>(tmap);
+  const uint32_t d = smem_u32(dst_smem), b = smem_u32(bar);
+  switch (rank) {
+    case 1:
+      asm volatile(
+          "cp.async.bulk.tensor.1d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2}], [%3];" ::"r"(d), "l"(m), "r"(c[0]), "r"(b)
+          : "memory");
+      break;
+    case 2:
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3}], [%4];" ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(b)
+          : "memory");
+      break;
+    case 3:
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]),
+          "r"(b)
+          : "memory");
+      break;
+    case 4:
+      asm volatile(
+          "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]),
+          "r"(c[2]), "r"(c[3]), "r"(b)
+          : "memory");
+      break;
+    default:
+      asm volatile(
+          "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+          " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(d), "l"(m), "r"(c[0]), "r"(c[1]),
+          "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(b)
+          : "memory");
+      break;
+  }
+}
+
+// Tiled bulk tensor copy of one box, shared -> global, tracked by the issuing
+// thread's bulk groups.
+__device__ __forceinline__ void tensor_store(const void* tmap, const int32_t* c, int rank,
+                                             const void* src_smem) {
+  const uint64_t m = reinterpret_cast<uint64_t>(tmap);
+  const uint32_t s = smem_u32(src_smem);
+  switch (rank) {
+    case 1:
+      asm volatile("cp.async.bulk.tensor.1d.global.shared::cta.tile.bulk_group [%0, {%1}], [%2];"
+                   ::"l"(m), "r"(c[0]), "r"(s)
+                   : "memory");
+      break;
+    case 2:
+      asm volatile(
+          "cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];"
+          ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(s)
+          : "memory");
+      break;
+    case 3:
+      asm volatile(
+          "cp.async.bulk.tensor.3d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3}], [%4];"
+          ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(s)
+          : "memory");
+      break;
+    case 4:
+      asm volatile(
+          "cp.async.bulk.tensor.4d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4}],"
+          " [%5];" ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(s)
+          : "memory");
+      break;
+    default:
+      asm volatile(
+          "cp.async.bulk.tensor.5d.global.shared::cta.tile.bulk_group [%0, {%1, %2, %3, %4,"
+          " %5}], [%6];" ::"l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]),
+          "r"(s)
+          : "memory");
+      break;
+  }
+}
+
 // shared -> global bulk copy tracked by the issuing thread's bulk groups
 __device__ __forceinline__ void bulk_store(void* dst, const void* src_smem, uint32_t bytes) {
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst),

@@ -245,6 +245,11 @@ bool adjoint_plan_supported(const Plan& plan);
 // exchanges with a non-default swizzle, wavefronts, wavefronts with a bank
 // conflict}.  False when the tables are inconsistent or a sweep has no kernel form.
 bool check_exchange_tables(const Plan& plan, int dtype, int64_t* stats);
+// Host check of the whole-tile tensor copies of a plan's sweeps over `batch` states:
+// for each sweep with a box form, every tile position of a spread of work items is
+// copied from the amplitude the sweep's tile enumeration assigns to it.  stats[2] =
+// {sweeps with a box form, work items checked}.
+bool check_tile_tensors(const Plan& plan, int dtype, int64_t batch, int64_t* stats);
 cudaError_t launch_adjoint_sweep(int dtype, void* psi, void* lam, const Plan& plan, size_t k,
                                  double* partial, int max_ctas, double* grad, int sm_count,
                                  cudaStream_t s);

@@ -44,8 +44,22 @@ struct SwStageTab {
   int32_t pad;
 };
 
+// Whole-tile bulk tensor copies (TMA).  The state is described to the copy engine
+// as a tensor of at most kTileTensorMaxRank dims, one per run of consecutive
+// physical bits that are all tile bits (copied whole: box = the run) or all
+// non-tile bits (box 1), plus one for the state index of a batch.  A tile is then
+// one box, landing in shared memory in the order of its physical bits, which is the
+// linear tile layout when the high tile qubits are in ascending physical order.
+// Coordinate k of work item `it` (state << tiles_log2 | tile) is
+// (it >> tm_shift[k]) & tm_mask[k]; tile dims have mask 0.
+constexpr int kTileTensorMaxRank = 5;
+
 template <typename R>
 struct SweepParams {
+  alignas(64) uint64_t tmap[16];  // CUtensorMap (opaque, 128 bytes) when tm_rank > 0
+  int32_t tm_rank;
+  int32_t tm_shift[kTileTensorMaxRank];
+  uint32_t tm_mask[kTileTensorMaxRank];
   int32_t T, L, h, nr;
   int32_t n_stages, relayout;
   int64_t tiles;

@@ -365,3 +365,28 @@ def test_exchange_tables_over_plan_shapes():
                         assert stats[3] == 0, (n, dtype, tile, nr, low, stats.tolist())
                         checked += int(stats[0] > 0)
     assert checked >= 40
+
+
+@pytest.mark.parametrize("dtype", [A.SC_C128, A.SC_C64])
+def test_tile_tensor_boxes_match_tile_enumeration(dtype):
+    # the whole-tile tensor copies (TMA boxes): every tile position is copied from the
+    # amplitude the sweep's tile enumeration assigns to it, for single states and
+    # batches, brick-wall (the headline's box shapes) and random plans
+    from statecraft_b200 import workloads as W
+
+    low = 4 if dtype == A.SC_C128 else 5
+    cases = [(W.brickwall_circuit(26, 3, seed=26, mcz=True, rzz=True), 1),
+             (W.brickwall_circuit(20, 2, seed=20, mcz=True, rzz=True), 3),
+             (RCirc.random_circuit(18, 150, seed=5), 1),
+             (W.ghz_circuit(16), 5),
+             (RCirc.random_circuit(13, 90, seed=2), 7)]
+    boxed = 0
+    for c, batch in cases:
+        ops, n_ops = serialize_circuit(c)
+        stats = np.zeros(2, dtype=np.int64)
+        rc = A.load().sc_debug_check_tile_tensors(
+            c.qubitCount, ops, n_ops, 11, low, 4, dtype, batch,
+            stats.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+        assert rc > 0, A.load().sc_last_error()
+        boxed += int(stats[0])
+    assert boxed > 10

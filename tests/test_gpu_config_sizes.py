@@ -10,9 +10,11 @@
   chunk.  The recursive-summation bound (Higham, Accuracy and Stability of Numerical
   Algorithms, 2nd ed., eq. 4.4) limits each to (terms summed) * 2^-53 * value, so at
   entry j of a 2^30-entry CDF the two can differ by up to (j + 2^11 + 2^19) * 2^-53
-  * cdf[j]; a draw closer than that to an entry can land on either side.  Reference
-  rules: StatevectorEngineTest.java:393-406 (1e-12), StatevectorEngine.java:229-338
-  (measurement).
+  * cdf[j]; a draw closer than that to an entry can land on either side.  With 2^30
+  entries of about 1e-9 each, the two sums' actual difference (1e-12 to 1e-11 here)
+  is a percent of an entry, so such draws are counted (at most 1 % of the shots) and
+  each must lie inside the band.  Reference rules: StatevectorEngineTest.java:393-406
+  (1e-12), StatevectorEngine.java:229-338 (measurement).
 - 26 qubits, complex128: the hardware-efficient ansatz of the adjoint workload
   (12 layers of RY, RZ and a CNOT ring, 624 angles, 64 random Pauli terms); <H>
   against the oracle, and the fused adjoint gradient on 8 angles against exact
@@ -111,7 +113,8 @@ def test_c2_30q_two_layers_state_and_counts_match_oracle():
             raise AssertionError((k, int(gpu_out[k]), j, float(u[k])))
         print("30q counts: shot %d drew %.17g, %.3e from a CDF entry (GPU %d, oracle %d)"
               % (k, u[k], min(abs(u[k] - cdf[j]), abs(u[k] - cdf[j - 1])), gpu_out[k], j))
-    assert len(mism) <= 2
+    print("30q counts: %d of %d outcomes differ, all at CDF entries" % (len(mism), shots))
+    assert len(mism) <= shots // 100
 
 
 def test_c4_26q_adjoint_gradient_vs_shift_and_differences():
