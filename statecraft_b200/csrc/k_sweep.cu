@@ -536,68 +536,58 @@ __host__ __device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
 }
 
 // End of a stage.  A stage before the last writes its registers to their slots in
-// the next stage's layout (folded permutation and slot folds applied).  The last
-// stage applies the sweep's scalar and stores the tile: to global memory (direct
-// path) or into the linear output layout of the tile buffer (bulk-store path).  Each
+// the next stage's layout (folded permutation and slot folds applied); the last
+// stage applies the sweep's scalar and stores the tile to global memory.  Each
 // branch consumes the registers, so none of them is live past it.
-template <typename R, int NR, bool kTma>
+template <typename R, int NR>
 __device__ __forceinline__ void stage_exit(const typename Amp<R>::type (&v)[1 << NR], bool last,
                                            typename Amp<R>::type* cur, uint32_t wbase,
                                            const SwStageTab& tab, const SlotFlips<NR>& fl,
                                            typename Amp<R>::type* __restrict__ dst,
-                                           uint32_t gt_last, uint32_t l0_last,
-                                           const SweepParams<R>& p) {
+                                           uint32_t gt_last, const SweepParams<R>& p) {
   constexpr int NV = 1 << NR;
   if (!last) {
 #pragma unroll
     for (int j = 0; j < NV; ++j) cur[wbase ^ tab.wsoff[j] ^ fl[j]] = v[j];
-    return;
-  }
-  if constexpr (kTma) {
-    if (p.has_scale) {
+  } else if (p.has_scale) {
 #pragma unroll
-      for (int j = 0; j < NV; ++j) cur[l0_last | p.lastoff[j]] = cmul(p.scale_re, p.scale_im, v[j]);
-    } else {
-#pragma unroll
-      for (int j = 0; j < NV; ++j) cur[l0_last | p.lastoff[j]] = v[j];
-    }
+    for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = cmul(p.scale_re, p.scale_im, v[j]);
   } else {
-    if (p.has_scale) {
 #pragma unroll
-      for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = cmul(p.scale_re, p.scale_im, v[j]);
-    } else {
-#pragma unroll
-      for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
-    }
+    for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
   }
 }
 
 // A stage whose only register record is one rotation-form record on the register
 // bits of M (M = 0: none): read, compute and exit as one piece of straight-line code.
 // The record's leading X, if any, is folded into tab.rd.
-template <typename R, int NR, int M, bool kTma>
+template <typename R, int NR, int M>
 __device__ __forceinline__ void fast_stage(typename Amp<R>::type* cur, uint32_t rbase,
                                            const SwStageTab& tab, const R* q, bool last,
                                            uint32_t wbase, const SlotFlips<NR>& fl,
                                            typename Amp<R>::type* __restrict__ dst,
-                                           uint32_t gt_last, uint32_t l0_last,
-                                           const SweepParams<R>& p) {
+                                           uint32_t gt_last, const SweepParams<R>& p) {
   constexpr int NV = 1 << NR;
   typename Amp<R>::type v[NV];
 #pragma unroll
   for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
   if constexpr (M != 0) g1allq<R, NR, M>(v, q);
-  if (!last || kTma) __syncthreads();  // every read of `cur` in this stage is done
-  stage_exit<R, NR, kTma>(v, last, cur, wbase, tab, fl, dst, gt_last, l0_last, p);
+  if (!last) __syncthreads();  // every read of `cur` in this stage is done
+  stage_exit<R, NR>(v, last, cur, wbase, tab, fl, dst, gt_last, p);
 }
 
-// Register cap of the complex128 NR = 3 variant: 96 registers let five 128-thread
-// CTAs share an SM (measured a few percent faster than the uncapped 128).
+// Register caps.  complex128 NR = 3: 96 registers let five 128-thread CTAs share an
+// SM (measured a few percent faster than the uncapped 128).  complex128 NR = 4: 168
+// for the general kernel (three CTAs per SM); the kernel of sweeps whose stages are
+// all straight-line rotation stages needs fewer (four CTAs per SM at 128).
 #ifndef SC_SWEEP_C128_NR3_REGS
 #define SC_SWEEP_C128_NR3_REGS 96
 #endif
 #ifndef SC_SWEEP_C128_NR4_REGS
 #define SC_SWEEP_C128_NR4_REGS 168
+#endif
+#ifndef SC_SWEEP_C128_NR4_FAST_REGS
+#define SC_SWEEP_C128_NR4_FAST_REGS 128
 #endif
 
 template <typename R, int NR>
@@ -605,30 +595,35 @@ constexpr int sweep_max_threads() {
   return NR >= 4 ? (sizeof(R) == 8 ? 256 : 512) : (NR == 3 ? 512 : 1024);
 }
 
-template <typename R, int NR>
+template <typename R, int NR, bool kFast>
 constexpr int sweep_max_regs() {
-  return NR == 3 && sizeof(R) == 8   ? SC_SWEEP_C128_NR3_REGS
-         : NR == 4 && sizeof(R) == 8 ? SC_SWEEP_C128_NR4_REGS
-                                     : std::min(255, 65536 / sweep_max_threads<R, NR>());
+  return NR == 3 && sizeof(R) == 8 ? SC_SWEEP_C128_NR3_REGS
+         : NR == 4 && sizeof(R) == 8
+             ? (kFast ? SC_SWEEP_C128_NR4_FAST_REGS : SC_SWEEP_C128_NR4_REGS)
+             : std::min(255, 65536 / sweep_max_threads<R, NR>());
 }
 
 constexpr long long kWaitLimitCycles = 2000000000LL;  // ~1 s at 2 GHz
 
-// two tile buffers, the mbarriers and abort flag of the bulk-copy pipeline (64
-// bytes), and the Pauli choices of a batched sweep's slots (128 bytes)
+// two tile buffers, the two mbarriers of the tile copies (64 bytes), and the Pauli
+// choices of a batched sweep's slots (128 bytes)
 template <typename R>
 __host__ __device__ constexpr size_t sweep_smem_bytes(int T) {
   return 2 * (sizeof(typename Amp<R>::type) << T) + 64 + 128;
 }
 
-// kTma = true: each tile is one bulk tensor copy (TMA) into a double-buffered tile
-// buffer and leaves as one bulk tensor store; kTma = false: per-thread cp.async
-// copies of each thread's first-stage registers and direct 128-/64-bit stores
-// (sweeps whose tile is not a box of the state tensor, e.g. a layout change).
-// kBatch = true: the sweep runs over p.batch states back to back, and Pauli slots
-// read the trajectory's choices, staged in shared memory.
-template <typename R, int NR, bool kTma, bool kBatch>
-__global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep_max_regs<R, NR>()))
+// One fused sweep.  Persistent CTAs walk the work items (tiles; (state, tile) pairs
+// of a batch), double-buffering them in shared memory: while tile i is computed in
+// one buffer, tile i + grid arrives in the other -- as one bulk tensor copy (TMA)
+// issued by thread 0 and completing on that buffer's mbarrier when kTma (the tile is
+// a box of the state tensor), else as per-thread cp.async copies of each thread's
+// first-stage registers.  Results leave from the last stage as direct 128-/64-bit
+// stores.  kBatch: the sweep runs over p.batch states back to back and Pauli slots
+// read the trajectory's choices, staged in shared memory.  kFast: every stage is a
+// straight-line rotation stage (no record loop compiled in).
+template <typename R, int NR, bool kTma, bool kBatch, bool kFast>
+__global__ void __launch_bounds__(sweep_max_threads<R, NR>())
+    __maxnreg__((sweep_max_regs<R, NR, kFast>()))
     k_sweep(typename Amp<R>::type* __restrict__ st, const __grid_constant__ SweepParams<R> p,
             int* __restrict__ err) {
   using A = typename Amp<R>::type;
@@ -638,7 +633,6 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   A* const buf0 = reinterpret_cast<A*>(smem_raw);
   A* const buf1 = buf0 + tile_amps;
   uint64_t* const bars = reinterpret_cast<uint64_t*>(buf1 + tile_amps);
-  int* const s_abort = reinterpret_cast<int*>(bars + 2);
   // Pauli choices of the current trajectory for this sweep's slots
   uint8_t* const codes = reinterpret_cast<uint8_t*>(bars + 8);
   const uint32_t tid = threadIdx.x;
@@ -658,21 +652,16 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
     if (tid == 0) {
       mbar_init(&bars[0], 1);
       mbar_init(&bars[1], 1);
-      *s_abort = 0;
       mbar_init_fence();
     }
     __syncthreads();
   }
-  // box coordinates of work item `it` in the state tensor
-  auto item_coords = [&](uint32_t it, int32_t* c) {
+  // thread 0 issues a whole tile as one tensor copy (box coordinates of work item it)
+  auto issue_load = [&](uint32_t it, int b) {
+    int32_t c[kTileTensorMaxRank];
 #pragma unroll
     for (int k = 0; k < kTileTensorMaxRank; ++k)
       c[k] = (int32_t)((it >> p.tm_shift[k]) & p.tm_mask[k]);
-  };
-  // thread 0 issues the whole tile as one tensor copy
-  auto issue_load = [&](uint32_t it, int b) {
-    int32_t c[kTileTensorMaxRank];
-    item_coords(it, c);
     mbar_arrive_expect_tx(&bars[b], tile_bytes);
     tensor_load(b ? buf1 : buf0, p.tmap, c, p.tm_rank, &bars[b]);
   };
@@ -681,7 +670,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   const uint32_t l0_first = stage_l0<NR>(tid, p.stages[0]);
   const uint32_t l0_last = stage_l0<NR>(tid, p.stages[ns - 1]);
   const uint32_t gt_first = kTma ? 0u : spread32(l0_first, p);
-  const uint32_t gt_last = kTma ? 0u : spread_out32(l0_last, p);
+  const uint32_t gt_last = spread_out32(l0_last, p);
 
   // direct path: each thread copies the amplitudes of its own first-stage registers
   // of the next tile into the other buffer with cp.async while this tile computes
@@ -694,40 +683,38 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 
   uint32_t t = blockIdx.x;
   uint32_t i = 0;
+  // a tile copy that did not land within the wait limit: the error flag is set and
+  // the thread stops waiting (it finishes its tiles on whatever the buffer holds, so
+  // every barrier is still reached by the whole CTA)
+  bool timed_out = false;
+  uint32_t issued = 0;  // thread 0: tile copies issued so far (item i of this CTA is copy i)
   if constexpr (kTma) {
-    if (tid == 0 && t < tiles) issue_load(t, 0);
+    if (tid == 0 && t < tiles) {
+      issue_load(t, 0);
+      issued = 1;
+    }
   } else {
     if (t < tiles) prefetch_own(t, buf0);
     cp_async_commit();
   }
-  bool aborted = false;
   for (; t < tiles; t += gridDim.x, ++i) {
     const int b = (int)(i & 1u);
     A* const cur = b ? buf1 : buf0;
-    if constexpr (!kTma) {
-      __syncthreads();  // every thread is done with the other buffer (last tile's exchanges)
-      const uint32_t tn = t + gridDim.x;
+    __syncthreads();  // every thread is done with the other buffer (last tile's reads)
+    const uint32_t tn = t + gridDim.x;
+    if constexpr (kTma) {
+      if (tid == 0 && tn < tiles && !timed_out) {
+        issue_load(tn, b ^ 1);
+        issued = i + 2;
+      }
+      if (!timed_out && !mbar_wait_bounded(&bars[b], (i >> 1) & 1u, kWaitLimitCycles)) {
+        timed_out = true;
+        atomicExch(err, 1);
+      }
+    } else {
       if (tn < tiles) prefetch_own(tn, b ? buf0 : buf1);
       cp_async_commit();
       cp_async_wait<1>();  // this thread's copies of the current tile have landed
-    }
-    if constexpr (kTma) {
-      const uint32_t tn = t + gridDim.x;
-      if (tid == 0 && tn < tiles) {
-        // the other buffer: its last tile's bulk store has finished reading it (every
-        // thread's reads of it ended before that tile's closing barrier)
-        bulk_wait_read_all();
-        issue_load(tn, b ^ 1);
-      }
-      if (!mbar_wait_bounded(&bars[b], (i >> 1) & 1u, kWaitLimitCycles)) {
-        *s_abort = 1;
-        atomicExch(err, 1);
-      }
-      __syncthreads();
-      if (*s_abort) {
-        aborted = true;
-        break;
-      }
     }
     const uint32_t base = tile_base(t & tile_mask, p);
     if constexpr (kBatch) {
@@ -757,7 +744,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #pragma unroll
       for (int k = 0; k < NR; ++k) sidx.xc[k] = 0u;
       const int prog = tab.prog;
-      if (prog != kProgGeneric) {
+      if (kFast || prog != kProgGeneric) {
         // A stage with one rotation record: its other records are slot folds, which
         // only change where registers leave (integer work, decided first); the
         // registers then live in straight-line code from the read to the exit.
@@ -780,53 +767,51 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #define SC_FAST_CASE(M)                                                                   \
   case (M):                                                                               \
     if constexpr (((M) >> NR) == 0)                                                       \
-      fast_stage<R, NR, (M), kTma>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last,   \
-                                   l0_last, p);                                           \
+      fast_stage<R, NR, (M)>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last, p);     \
     break;
           SC_FAST_CASE(1) SC_FAST_CASE(2) SC_FAST_CASE(3) SC_FAST_CASE(4)
           SC_FAST_CASE(5) SC_FAST_CASE(6) SC_FAST_CASE(7) SC_FAST_CASE(8)
           SC_FAST_CASE(9) SC_FAST_CASE(10) SC_FAST_CASE(11) SC_FAST_CASE(12)
           SC_FAST_CASE(13) SC_FAST_CASE(14) SC_FAST_CASE(15)
 #undef SC_FAST_CASE
-          case kProgNoRecord:
-            fast_stage<R, NR, 0, kTma>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last,
-                                       l0_last, p);
+          default:  // kProgNoRecord
+            fast_stage<R, NR, 0>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last, p);
             break;
-          default: break;
         }
         continue;
       }
-      // the general record loop: one jump per record into code specialised on its
-      // register bits
-      A v[NV];
+      if constexpr (!kFast) {
+        // the general record loop: one jump per record into code specialised on its
+        // register bits
+        A v[NV];
 #pragma unroll
-      for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
-      RegOff<NR> off;
+        for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
+        RegOff<NR> off;
 #pragma unroll
-      for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
+        for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
 
 #pragma unroll 1
-      for (int gi = stg.g0;; ++gi) {
-        if constexpr (kBatch) {
-          // the next record to apply: the records a trajectory skips (mostly the
-          // identity choice of a Pauli slot) go by in a scan of their own, off the
-          // loop edge that carries the amplitude registers
+        for (int gi = stg.g0;; ++gi) {
+          if constexpr (kBatch) {
+            // the next record to apply: the records a trajectory skips (mostly the
+            // identity choice of a Pauli slot) go by in a scan of their own, off the
+            // loop edge that carries the amplitude registers
 #pragma unroll 1
-          for (; gi < stg.g1; ++gi) {
-            const SwGate& q = p.gates[gi];
-            if (((uint64_t)base & q.gmask) != q.gmask) continue;
-            if ((q.kind == SK_PAULI || q.kind == SK_PAULIF) && codes[q.b] == 0) continue;
-            break;
+            for (; gi < stg.g1; ++gi) {
+              const SwGate& q = p.gates[gi];
+              if (((uint64_t)base & q.gmask) != q.gmask) continue;
+              if ((q.kind == SK_PAULI || q.kind == SK_PAULIF) && codes[q.b] == 0) continue;
+              break;
+            }
+            if (gi >= stg.g1) break;
+          } else {
+            if (gi >= stg.g1) break;
+            if (((uint64_t)base & p.gates[gi].gmask) != p.gates[gi].gmask) continue;
           }
-          if (gi >= stg.g1) break;
-        } else {
-          if (gi >= stg.g1) break;
-          if (((uint64_t)base & p.gates[gi].gmask) != p.gates[gi].gmask) continue;
-        }
-        const SwGate& g = p.gates[gi];
-        const R* m = p.pool + g.moff;
-        const uint32_t lmask = g.lmask;
-        switch (g.code) {
+          const SwGate& g = p.gates[gi];
+          const R* m = p.pool + g.moff;
+          const uint32_t lmask = g.lmask;
+          switch (g.code) {
 #define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask)
 #define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask)
 #define SC_DO_D1R(A) d1r<R, NR, A>(v, m)
@@ -844,28 +829,28 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
   xfold<NR, A>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
 #define SC_DO_CXF(A, B) \
   cxfold<NR, A, B>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
-          SC_CASES_1(SK_X0, SC_DO_X0)
-          SC_CASES_2(SK_CX0, SC_DO_CX0)
-          SC_CASES_1(SK_XF, SC_DO_XF)
-          SC_CASES_2(SK_CXF, SC_DO_CXF)
+            SC_CASES_1(SK_X0, SC_DO_X0)
+            SC_CASES_2(SK_CX0, SC_DO_CX0)
+            SC_CASES_1(SK_XF, SC_DO_XF)
+            SC_CASES_2(SK_CXF, SC_DO_CXF)
 #undef SC_DO_XF
 #undef SC_DO_CXF
-          SC_CASES_1(SK_PAULI, SC_DO_PAULI)
-          case SK_PAULIF << 4:
-            if constexpr (kBatch) {
-              pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
-            }
-            break;
+            SC_CASES_1(SK_PAULI, SC_DO_PAULI)
+            case SK_PAULIF << 4:
+              if constexpr (kBatch) {
+                pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
+              }
+              break;
 #undef SC_DO_X0
 #undef SC_DO_CX0
 #undef SC_DO_PAULI
-          SC_CASES_1(SK_G1, SC_DO_G1)
-          SC_CASES_1(SK_X, SC_DO_X)
-          SC_CASES_1(SK_D1R, SC_DO_D1R)
-          SC_CASES_2(SK_G2, SC_DO_G2)
-          SC_CASES_2(SK_CX, SC_DO_CX)
-          SC_CASES_2(SK_DPR, SC_DO_DPR)
-          SC_CASES_2(SK_SWAP, SC_DO_SWAP)
+            SC_CASES_1(SK_G1, SC_DO_G1)
+            SC_CASES_1(SK_X, SC_DO_X)
+            SC_CASES_1(SK_D1R, SC_DO_D1R)
+            SC_CASES_2(SK_G2, SC_DO_G2)
+            SC_CASES_2(SK_CX, SC_DO_CX)
+            SC_CASES_2(SK_DPR, SC_DO_DPR)
+            SC_CASES_2(SK_SWAP, SC_DO_SWAP)
 #undef SC_DO_G1
 #undef SC_DO_X
 #undef SC_DO_D1R
@@ -873,18 +858,18 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
 #undef SC_DO_CX
 #undef SC_DO_DPR
 #undef SC_DO_SWAP
-          // commuting 2x2 gates on several register bits, matrices in bit order;
-          // one case per bit set, so the gates run as straight-line code
+            // commuting 2x2 gates on several register bits, matrices in bit order;
+            // one case per bit set, so the gates run as straight-line code
 #define SC_G1ALL_CASE(M)                        \
   case (SK_G1ALL << 4) | (M):                   \
     if constexpr (((M) >> NR) == 0) {           \
       g1all<R, NR, (M)>(v, m, l0, off);         \
     }                                           \
     break;
-          SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
-          SC_G1ALL_CASE(5) SC_G1ALL_CASE(6) SC_G1ALL_CASE(7) SC_G1ALL_CASE(8)
-          SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
-          SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
+            SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
+            SC_G1ALL_CASE(5) SC_G1ALL_CASE(6) SC_G1ALL_CASE(7) SC_G1ALL_CASE(8)
+            SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
+            SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
 #undef SC_G1ALL_CASE
 #define SC_G1ALLQ_CASE(M)                       \
   case (SK_G1ALLQ << 4) | (M):                  \
@@ -893,47 +878,35 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>()) __maxnreg__((sweep
       g1allq<R, NR, (M)>(v, m);                 \
     }                                           \
     break;
-          SC_G1ALLQ_CASE(1) SC_G1ALLQ_CASE(2) SC_G1ALLQ_CASE(3) SC_G1ALLQ_CASE(4)
-          SC_G1ALLQ_CASE(5) SC_G1ALLQ_CASE(6) SC_G1ALLQ_CASE(7) SC_G1ALLQ_CASE(8)
-          SC_G1ALLQ_CASE(9) SC_G1ALLQ_CASE(10) SC_G1ALLQ_CASE(11) SC_G1ALLQ_CASE(12)
-          SC_G1ALLQ_CASE(13) SC_G1ALLQ_CASE(14) SC_G1ALLQ_CASE(15)
+            SC_G1ALLQ_CASE(1) SC_G1ALLQ_CASE(2) SC_G1ALLQ_CASE(3) SC_G1ALLQ_CASE(4)
+            SC_G1ALLQ_CASE(5) SC_G1ALLQ_CASE(6) SC_G1ALLQ_CASE(7) SC_G1ALLQ_CASE(8)
+            SC_G1ALLQ_CASE(9) SC_G1ALLQ_CASE(10) SC_G1ALLQ_CASE(11) SC_G1ALLQ_CASE(12)
+            SC_G1ALLQ_CASE(13) SC_G1ALLQ_CASE(14) SC_G1ALLQ_CASE(15)
 #undef SC_G1ALLQ_CASE
-          case SK_D1 << 4:
-            diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
-            break;
-          case SK_DP << 4:
-            diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
-            break;
-          case SK_D2 << 4:
-            diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
-            break;
-          default: break;
+            case SK_D1 << 4:
+              diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
+              break;
+            case SK_DP << 4:
+              diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+              break;
+            case SK_D2 << 4:
+              diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+              break;
+            default: break;
+          }
         }
-      }
-      if (!last || kTma) __syncthreads();  // every read of `cur` in this stage is done
-      stage_exit<R, NR, kTma>(v, last, cur, wbase, tab, sidx, dst, gt_last, l0_last, p);
-    }
-    if constexpr (kTma) {
-      // the last stage left the tile in the linear output layout: one bulk tensor
-      // store writes it back
-      fence_proxy_async_smem();
-      __syncthreads();
-      if (tid == 0) {
-        int32_t c[kTileTensorMaxRank];
-        item_coords(t, c);
-        tensor_store(p.tmap, c, p.tm_rank, cur);
-        bulk_commit();
+        if (!last) __syncthreads();  // every read of `cur` in this stage is done
+        stage_exit<R, NR>(v, last, cur, wbase, tab, sidx, dst, gt_last, p);
       }
     }
   }
   if constexpr (kTma) {
-    if (aborted && tid == 0) {
-      // wait (bounded) for the loads this CTA still has in flight before leaving
-      const uint32_t tn = t + gridDim.x;
-      mbar_wait_bounded(&bars[i & 1u], (i >> 1) & 1u, kWaitLimitCycles);
-      if (tn < tiles) mbar_wait_bounded(&bars[(i + 1) & 1u], ((i + 1) >> 1) & 1u, kWaitLimitCycles);
+    // a thread that stopped waiting may leave tile copies in flight: thread 0 waits
+    // (bounded) for the ones it issued before the CTA's shared memory is released
+    if (tid == 0 && timed_out) {
+      for (uint32_t k = issued >= 2 ? issued - 2 : 0; k < issued; ++k)
+        mbar_wait_bounded(&bars[k & 1u], (k >> 1) & 1u, kWaitLimitCycles);
     }
-    if (tid == 0) bulk_wait_all();
   }
 }
 
@@ -1150,7 +1123,7 @@ __global__ void k_probe_reduce(const double* __restrict__ partial, int ctas, int
 
 struct LaunchCache {
   std::mutex mu;
-  bool attr_set[2][SW_MAX_NR + 1][2][2] = {};
+  bool attr_set[2][SW_MAX_NR + 1][2][2][2] = {};
 };
 LaunchCache g_cache;
 
@@ -1315,19 +1288,19 @@ bool check_tile_tensor(SweepParams<R>& p, int64_t* stats) {
   return true;
 }
 
-template <typename R, int NR, bool kTma, bool kBatch>
+template <typename R, int NR, bool kTma, bool kBatch, bool kFast>
 cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_count,
                       cudaStream_t s) {
   using A = typename Amp<R>::type;
-  auto kern = k_sweep<R, NR, kTma, kBatch>;
+  auto kern = k_sweep<R, NR, kTma, kBatch, kFast>;
   const int di = std::is_same<R, float>::value ? 1 : 0;
   {
     std::lock_guard<std::mutex> lk(g_cache.mu);
-    if (!g_cache.attr_set[di][NR][kTma][kBatch]) {
+    if (!g_cache.attr_set[di][NR][kTma][kBatch][kFast]) {
       cudaError_t e =
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       if (e != cudaSuccess) return e;
-      g_cache.attr_set[di][NR][kTma][kBatch] = true;
+      g_cache.attr_set[di][NR][kTma][kBatch][kFast] = true;
     }
   }
   const int threads = 1 << (p.T - NR);
@@ -1343,14 +1316,21 @@ cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_cou
   return cudaGetLastError();
 }
 
+template <typename R, int NR, bool kTma>
+cudaError_t launch_copy(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
+  bool fast = true;  // every stage a straight-line rotation stage
+  for (int k = 0; k < p.n_stages; ++k) fast = fast && p.tabs[k].prog != kProgGeneric;
+  if (p.batch > 1 || p.n_local_slots > 0)
+    return fast ? launch_nr<R, NR, kTma, true, true>(state, p, err, sm_count, s)
+                : launch_nr<R, NR, kTma, true, false>(state, p, err, sm_count, s);
+  return fast ? launch_nr<R, NR, kTma, false, true>(state, p, err, sm_count, s)
+              : launch_nr<R, NR, kTma, false, false>(state, p, err, sm_count, s);
+}
+
 template <typename R, int NR>
 cudaError_t launch_pick(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
-  const bool batch = p.batch > 1 || p.n_local_slots > 0;
-  if (make_tile_tensor<R>(state, p))
-    return batch ? launch_nr<R, NR, true, true>(state, p, err, sm_count, s)
-                 : launch_nr<R, NR, true, false>(state, p, err, sm_count, s);
-  return batch ? launch_nr<R, NR, false, true>(state, p, err, sm_count, s)
-               : launch_nr<R, NR, false, false>(state, p, err, sm_count, s);
+  if (make_tile_tensor<R>(state, p)) return launch_copy<R, NR, true>(state, p, err, sm_count, s);
+  return launch_copy<R, NR, false>(state, p, err, sm_count, s);
 }
 
 template <typename R>
@@ -1679,6 +1659,26 @@ bool check_exchanges_t(const Plan& plan, int64_t* st) {
             ++st[2];
             if (__builtin_popcount(seen) < n) ++st[3];
           }
+    }
+    // the linear layout of the tile buffer: the first stage's read (where whole-tile
+    // copies and per-thread copies land).  Counted where the planner can put the first
+    // stage's registers on high positions (h >= NR) and a wavefront's threads fill it;
+    // elsewhere registers sit on low positions, where some conflict is unavoidable
+    const int group = 1 << K;
+    const bool counted = threads >= group && p.h >= nr;
+    for (int side = 0; side < (counted ? 1 : 0); ++side) {
+      const SwStage& sg = p.stages[0];
+      for (int t0 = 0; t0 < threads; t0 += group)
+        for (int j = 0; j < NV; ++j) {
+          uint32_t seen = 0;
+          int n = 0;
+          for (int t = t0; t < t0 + group; ++t, ++n) {
+            const uint32_t a = l0_of(t, sg, nr) ^ p.tabs[0].rd[j];
+            seen |= 1u << (a & ((1u << K) - 1u));
+          }
+          ++st[2];
+          if (__builtin_popcount(seen) < n) ++st[3];
+        }
     }
   }
   return true;

@@ -141,7 +141,8 @@ def test_c4_26q_adjoint_gradient_vs_shift_and_differences():
         eng.close()
     print("26q adjoint: |grad - shift| = %.3e, |grad - FD| = %.3e"
           % (np.max(np.abs(grad[picks] - shift)), np.max(np.abs(grad[picks] - fd))))
-    assert np.max(np.abs(grad[picks])) > 1e-3  # a gradient that is not trivially zero
+    # random 64-term Pauli sums on 26 qubits have small gradients (about 1e-4)
+    assert np.max(np.abs(grad[picks])) > 1e-5  # a gradient that is not trivially zero
     np.testing.assert_allclose(grad[picks], shift, rtol=0, atol=1e-8)
     np.testing.assert_allclose(grad[picks], fd, rtol=0, atol=1e-8)
     # <H> of the forward pass against the oracle's state
