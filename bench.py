@@ -12,7 +12,7 @@ Metric: gate-level amplitude updates per second (1.643e12 per step).
 N > 1 runs N independent replicas (one process per GPU under torchrun, weak
 scaling); the state vector of one circuit does not shard without an exchange.
 `--impl reference` times the CPU restatement of the reference engine (the Java
-engine cannot run here) on a bounded sample of the same workload.
+engine cannot run here: no JDK) on a bounded sample of the same 30-qubit workload.
 """
 from __future__ import annotations
 
@@ -33,8 +33,6 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "amp-updates/s (30q c128 brick-wall depth 40 + MCZ29 + RZZ, fused, countsAll 8192)"
 UNIT = "amp-updates/s"
-CPU_QUBITS = 26   # bounded CPU sample: same generator, fewer qubits / layers
-CPU_LAYERS = 8
 
 
 def parse_args(argv=None):
@@ -50,11 +48,11 @@ def parse_args(argv=None):
     ap.add_argument("--sweep-budget", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["statevector", "qaoa", "adjoint", "trajectories"],
+    ap.add_argument("--workload", choices=["statevector", "c1", "qaoa", "adjoint", "trajectories"],
                     default="statevector",
-                    help="statevector: the headline line; the others time the batched "
-                         "QAOA, adjoint-gradient and noisy-trajectory workloads (one JSON "
-                         "line each, 1 GPU)")
+                    help="statevector: the headline line; c1: the 20-qubit plain drop-in; "
+                         "the others time the batched QAOA, adjoint-gradient and "
+                         "noisy-trajectory workloads (one JSON line each, 1 GPU)")
     ap.add_argument("--instances", type=int, default=4096, help="QAOA batch size")
     ap.add_argument("--trajectories", type=int, default=1024, help="trajectory batch size")
     ap.add_argument("--no-tune", action="store_true", help="QAOA: fixed kernel shape")
@@ -133,50 +131,110 @@ def ncu_traffic() -> dict:
 # ---------------------------------------------------------------------------
 # CPU baseline (the oracle restatement of the reference engine, OpenMP)
 # ---------------------------------------------------------------------------
-def cpu_baseline(seconds_budget: float = 30.0) -> dict:
-    from oracle import oracle as O
-    from statecraft_b200 import workloads as W
-    from statecraft_b200.engine import serialize_circuit
+_NATIVE_ORACLE = None
 
-    cores = len(os.sched_getaffinity(0))
-    c = W.brickwall_circuit(CPU_QUBITS, CPU_LAYERS, seed=3030, mcz=True, rzz=True)
-    ops, n_ops = serialize_circuit(c)
-    st = O.initial_state(CPU_QUBITS)
-    t0 = time.perf_counter()
-    rc, _ = O.run(CPU_QUBITS, ops, n_ops, st)
-    dt = time.perf_counter() - t0
-    assert rc == 0
-    return {"value": W.amp_updates(c) / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "seconds": dt,
-            "sample": (f"C restatement of StatevectorEngine (per-gate sweeps, OpenMP {cores} threads, "
-                       f"-O2) on the same brick-wall generator at {CPU_QUBITS} qubits x {CPU_LAYERS} "
-                       f"layer(s) ({n_ops} ops); the Java engine is unavailable on this host")}
+
+def native_oracle():
+    """The oracle's C restatement built with -O3 -march=native for the host that runs
+    the bench (compiled here, into a temporary directory, because the library in
+    oracle/_build is built -O2 for any x86-64); same -ffp-contract=off arithmetic."""
+    global _NATIVE_ORACLE
+    if _NATIVE_ORACLE is None:
+        import ctypes
+
+        from statecraft_b200 import _abi as A
+
+        out = Path(tempfile.mkdtemp(prefix="sc_oracle_native_")) / "libsc_oracle_native.so"
+        cc = "/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc"
+        subprocess.run([cc, "-O3", "-march=native", "-ffp-contract=off", "-fno-fast-math",
+                        "-fPIC", "-fopenmp", "-std=c11", "-shared", "-o", str(out),
+                        str(ROOT / "oracle" / "sc_oracle.c"), "-lm"], check=True)
+        lib = ctypes.CDLL(str(out))
+        lib.scx_apply_op.restype = ctypes.c_int
+        lib.scx_apply_op.argtypes = [ctypes.POINTER(ctypes.c_double), ctypes.c_int,
+                                     ctypes.POINTER(A.ScOp), ctypes.POINTER(ctypes.c_double),
+                                     ctypes.c_int64]
+        _NATIVE_ORACLE = lib
+    return _NATIVE_ORACLE
+
+
+class CpuSample:
+    """A bounded CPU sample of the headline workload: the first `n_ops` operations of
+    the 30-qubit brick-wall generator (seed 3030, MCZ + RZZ), applied one full-state
+    pass each by the oracle's restatement of the reference engine's per-gate loops
+    (StatevectorOps.java), on one pre-touched 16 GiB state reused between samples."""
+
+    def __init__(self, qubits: int = 30, n_ops: int = 47):
+        import ctypes
+
+        from statecraft_b200 import quantum as Q
+        from statecraft_b200 import workloads as W
+        from statecraft_b200.engine import serialize_circuit
+
+        self.qubits = qubits
+        c = W.brickwall_circuit(qubits, 1, seed=3030, mcz=True, rzz=True)
+        self.circuit = Q.QuantumCircuit(qubits, tuple(c.operations[:n_ops]))
+        self.ops, self.n_ops = serialize_circuit(self.circuit)
+        self.updates = W.amp_updates(self.circuit)
+        self.state = np.zeros(2 << qubits)
+        self.state[0] = 1.0
+        self.state[1::4096] = 0.0  # touch every page once before timing
+        self.lib = native_oracle()
+        self._dp = self.state.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        self.cores = len(os.sched_getaffinity(0))
+
+    def run(self) -> float:
+        """Seconds for one pass over the sample's operations."""
+        import ctypes
+
+        from statecraft_b200 import _abi as A
+
+        base = ctypes.addressof(self.ops)
+        t0 = time.perf_counter()
+        for i in range(self.n_ops):
+            op = ctypes.cast(base + i * ctypes.sizeof(A.ScOp), ctypes.POINTER(A.ScOp))
+            rc = self.lib.scx_apply_op(self._dp, self.qubits, op, None, 0)
+            assert rc == 0
+        return time.perf_counter() - t0
+
+    def describe(self) -> str:
+        return (f"C restatement of StatevectorEngine's per-gate loops (OpenMP {self.cores} threads, "
+                f"gcc -O3 -march=native -ffp-contract=off) on the first {self.n_ops} operations "
+                f"of the same {self.qubits}-qubit brick-wall generator (layer 0: U3 on every "
+                f"qubit, CNOT brick, MCZ, RZZ); the Java engine is unavailable on this host (no JDK)")
+
+
+def cpu_baseline() -> dict:
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    s = CpuSample()
+    s.run()  # warm-up pass
+    dt = s.run()
+    out = {"value": s.updates / dt, "unit": UNIT, "cores": s.cores, "kind": "port",
+           "seconds": dt, "sample": s.describe()}
+    del s
+    return out
 
 
 def run_reference(args, rank: int) -> None:
     if rank != 0:
         return
-    from statecraft_b200 import workloads as W
-
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
+    # each step: the first 10 operations of the 30-qubit workload (a few seconds on 16 cores)
+    s = CpuSample(n_ops=10)
     for _ in range(args.warmup):
-        cpu_baseline()
-    vals = []
-    t_all = 0.0
-    for _ in range(args.steps):
-        r = cpu_baseline()
-        vals.append(r["value"])
-        t_all += r["seconds"]
-    value = float(np.median(vals))
+        s.run()
+    secs = [s.run() for _ in range(args.steps)]
+    value = s.updates * args.steps / sum(secs)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 1e3 * t_all / args.steps, "higher_is_better": True,
+            "ms_per_step": 1e3 * sum(secs) / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"brick-wall U3+CNOT+MCZ+RZZ, {CPU_QUBITS} qubits x {CPU_LAYERS} "
-                                   f"layer(s) per step (bounded CPU sample of the 30q x 40 workload)",
-                       "qubits": CPU_QUBITS, "layers": CPU_LAYERS},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["cores"], "kind": "port",
-                             "sample": r["sample"]},
+            "config": {"workload": f"brick-wall U3+CNOT+MCZ+RZZ, {s.qubits} qubits, first "
+                                   f"{s.n_ops} operations per step (bounded CPU sample of the "
+                                   f"30q x 40 workload)",
+                       "qubits": s.qubits, "ops_per_step": s.n_ops},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": s.cores, "kind": "port",
+                             "sample": s.describe()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -333,6 +391,87 @@ def run_trajectories_bench(args) -> dict:
                          "frac": (gbs / peak) if gbs else None, "traffic": None}}
 
 
+def run_c1(args) -> dict:
+    """The 20-qubit plain drop-in: brick-wall U3 + CNOT, 20 layers, angles from
+    SplittableRandom(2020), |0..0> start, final state and countsAll(1024) with seed 42.
+    `value` times sc_run + sc_sample on the device (state resident); `e2e` times
+    StatevectorB200Engine.simulate with the final state (16 MiB) and the histogram
+    copied back.  The 16 MiB state fits in L2; a 512 MiB buffer is written between
+    timed steps so every step starts with L2 holding other data."""
+    import torch
+
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import (B200Config, MeasurementInstruction, NativeContext,
+                                        SimulationRequest, StatevectorB200Engine,
+                                        serialize_circuit)
+
+    n, layers, shots = 20, 20, 1024
+    circuit = W.brickwall_circuit(n, layers, seed=2020)
+    ops, n_ops = serialize_circuit(circuit)
+    updates = W.amp_updates(circuit)
+    qubits = list(range(n))
+    steps = max(args.steps, 1) * 50
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device="cuda")
+    ctx = NativeContext(B200Config(timing=True))
+    stream = torch.cuda.ExternalStream(ctx.lib.sc_stream(ctx.handle))
+
+    def step():
+        ctx.run_ops(n, ops, n_ops)
+        return ctx.sample(qubits, shots, 42)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    ctx.reset_kernel_stats()
+    total_ms = 0.0
+    with ClockSampler(0) as clk:
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(1)
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            b.synchronize()
+            total_ms += a.elapsed_time(b)
+    stats = ctx.kernel_stats()
+    plan = ctx.plan_stats()
+    ctx.close()
+    launches = sum(v["launches"] for v in stats.values())
+    engine = StatevectorB200Engine(B200Config())
+    req = SimulationRequest.zeroState(circuit).withMeasurement(
+        MeasurementInstruction.countsAll(shots).withSeed(42), True)
+    engine.simulate(req)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        res = engine.simulate(req)
+    e2e_s = (time.perf_counter() - t0) / steps
+    assert sum(res.measurement.counts.values()) == shots
+    engine.close()
+    ms = total_ms / steps
+    sw = stats.get("sweep", {"launches": 0, "ms": 0.0, "bytes": 0.0})
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    gbs = (sw["bytes"] / (sw["ms"] / 1e3) / 1e9) if sw["ms"] else None
+    return {"metric": "amp-updates/s (20q c128 brick-wall depth 20, final state + countsAll 1024)",
+            "value": updates / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "brick-wall U3+CNOT, 20 qubits x 20 layers, countsAll(1024) "
+                                   "seed 42, final state, c128", "qubits": n, "layers": layers,
+                       "angle_seed": 2020, "shots": shots, "amp_updates_per_step": updates,
+                       "sweeps_per_step": plan["sweeps"], "stages_per_step": plan["stages"],
+                       "l2": "state (16 MiB) fits in L2; a 512 MiB write between timed steps"},
+            "gpu_launches": launches // steps,
+            "kernel_stats": stats,
+            "e2e": {"value": updates / e2e_s, "unit": UNIT, "h2d_bytes_per_step": n_ops * 280,
+                    "d2h_bytes_per_step": (16 << n) + 4 * shots, "seconds_per_step": e2e_s},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                         "frac": (gbs / peak) if gbs else None, "traffic": None,
+                         "note": "sweeps of an L2-resident state: bytes per sweep over its time"},
+            "clocks": clk.summary()}
+
+
 # ---------------------------------------------------------------------------
 # the B200 engine
 # ---------------------------------------------------------------------------
@@ -345,7 +484,7 @@ def main(argv=None) -> int:
         run_reference(args, rank)
         return 0
     if args.workload != "statevector":
-        fn = {"qaoa": run_qaoa, "adjoint": run_adjoint,
+        fn = {"c1": run_c1, "qaoa": run_qaoa, "adjoint": run_adjoint,
               "trajectories": run_trajectories_bench}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return 0
@@ -475,7 +614,6 @@ def main(argv=None) -> int:
             "e2e": e2e,
             "clocks": clk.summary()}
     if world == 1 and not args.no_cpu_baseline:
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count() or 1))
         line["cpu_baseline"] = cpu_baseline()
     print(json.dumps(line), flush=True)
     return 0

@@ -1546,7 +1546,13 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
     tb.qoff = 0;
     tb.xm = 0;
     tb.pad = 0;
-    if (n_other == 0 && n_rot == 1) {
+    static const bool straight = [] {
+      const char* v = getenv("STATECRAFT_B200_FAST_STAGES");
+      return !(v && atoi(v) == 0);
+    }();
+    if (!straight) {
+      // every stage through the record loop
+    } else if (n_other == 0 && n_rot == 1) {
       tb.prog = plan.gates[rot_g].a & 15;
       tb.qoff = plan.gates[rot_g].moff - sw.pool0;
       tb.xm = plan.gates[rot_g].b & (nv - 1);
