@@ -229,7 +229,7 @@ SC_API int32_t sc_last_plan_stats(void* ctx, int64_t* sweeps, int64_t* gates, in
  * returns after the stream has finished.
  * Uniforms: d_uniforms[shot] (device, nullable) else SplittableRandom(seed).
  * Scratch is a fixed array in the library's device data sized for at most 2^30
- * amplitudes (30 qubits, about 8 MiB held by every GPU that loads the library);
+ * amplitudes (30 qubits, about 24 MiB held by every GPU that loads the library);
  * larger states return SC_EINVAL.  The first call on a device looks the array up
  * (make it before any stream capture); a cudaDeviceReset after that is not
  * supported.  All calls share the array: calls that overlap on the GPU race. */

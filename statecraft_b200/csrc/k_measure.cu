@@ -1,13 +1,29 @@
-// Measurement: marginal probabilities, FP64 prefix sums and per-shot search.
+// Measurement: marginal probabilities, the reference's running sum and per-shot search.
 //
 // Reference semantics (StatevectorEngine.java:229-338): probabilities over the
-// measured qubits, rescaled by 1/sum when |sum - 1| > 1e-12, running sum with the
-// last entry forced to 1.0, and per shot the first index whose cumulative value
-// is >= u (u >= 1 -> last index).  Here the cumulative array is never
-// materialised: pass A reduces chunks of CHUNK probabilities (FP64), pass B scans
-// the chunk sums in one CTA, pass C gives each shot a warp that binary-searches
-// the chunk prefixes and scans its chunk in FP64.  Uniforms are the reference's
-// SplittableRandom(seed).nextDouble() sequence, computed per shot from (seed, k).
+// measured qubits, rescaled by 1/sum when |sum - 1| > 1e-12 (the sum a left-to-right
+// FP64 sum), a left-to-right FP64 running sum with the last entry forced to 1.0, and
+// per shot the first index whose running sum is >= u (u >= 1 -> last index).
+// Uniforms are the reference's SplittableRandom(seed).nextDouble() sequence,
+// computed per shot from (seed, k).
+//
+// The running sum is reproduced bit for bit without a sequential pass over the whole
+// array.  While a running sum S stays in one binade [2^e, 2^(e+1)), S is an integer A
+// times ulp = 2^(e-52), and fl(S + p) = (A + round(p / ulp)) * ulp with round to
+// nearest, ties to even (IEEE 754 round-to-nearest-even restated on integers): the
+// result depends on A only through its parity, and only when p / ulp is exactly
+// half-way.  A run of additions therefore acts on A as "add d0 if A is even, d1 if
+// odd, and leave this parity", and such effects compose associatively.  Pass A sums
+// chunks of kChunk probabilities approximately (FP64); pass B turns them into
+// approximate running sums, which tell which chunks lie inside one binade (with a
+// margin far above the summation error); pass C computes each such chunk's effect in
+// integers; pass D walks the chunks in order from S = 0 -- one integer step per
+// clean chunk, element by element (exact FP64 adds) for the few chunks that cross a
+// binade, start near zero or end the array -- and records the exact running sum
+// before each chunk, the exact total and the rescaling decision; when the reference
+// rescales, passes A-D run again on the rescaled probabilities.  Pass E gives each
+// shot a warp that binary-searches the exact chunk starts and replays its chunk: lane
+// effects, a warp scan, then exact FP64 adds within each lane.
 #include <cfloat>
 
 #include "sc_device.cuh"
@@ -51,72 +67,313 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return s;  // valid in thread 0
 }
 
-// pass A: S[c] = sum of chunk c.  A batch of states of len_per entries each,
-// stored back to back, has chunks_per chunks per state (chunk c of the whole
-// array is chunk c % chunks_per of state c / chunks_per).
+// pass A: sums[c] = sum of chunk c.  A batch of states of len_per entries each,
+// stored back to back, has chunks_per chunks per state (chunk c of the whole array is
+// chunk c % chunks_per of state c / chunks_per).  With `sc`, only the states the
+// reference rescales are summed, over their rescaled probabilities.
 template <typename Src>
 __global__ void __launch_bounds__(kThreadsA) k_chunk_sums(Src src, uint64_t len_per,
                                                           uint64_t chunks_per, double* sums,
-                                                          uint64_t chunks) {
+                                                          uint64_t chunks,
+                                                          const SampleScalars* sc) {
   __shared__ double red[kThreadsA / 32];
   for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
     const uint64_t st = c / chunks_per;
+    if (sc && !sc[st].scaled) continue;
+    const double scale = sc ? sc[st].scale : 1.0;
     const uint64_t b = (c - st * chunks_per) * kChunk;
     const uint64_t off = st * len_per;
     double acc = 0.0;
     for (int k = threadIdx.x; k < kChunk; k += kThreadsA) {
       const uint64_t i = b + k;
-      if (i < len_per) acc += src(off + i);
+      if (i < len_per) acc += sc ? __dmul_rn(src(off + i), scale) : src(off + i);
     }
     const double s = block_sum<kThreadsA>(acc, red);
     if (threadIdx.x == 0) sums[c] = s;
   }
 }
 
-// pass B (one CTA of 1024 threads per state): total, scale, exclusive chunk prefixes
-__global__ void __launch_bounds__(1024) k_chunk_scan(const double* sums, uint64_t chunks,
-                                                     double* prefix, SampleScalars* out) {
+// pass B (one CTA of 1024 threads per state): approximate exclusive running sums of
+// the chunk sums
+__global__ void __launch_bounds__(1024) k_prefix_approx(const double* sums, uint64_t chunks,
+                                                        double* prefix, const SampleScalars* sc) {
+  if (sc && !sc[blockIdx.x].scaled) return;
   sums += blockIdx.x * chunks;
   prefix += blockIdx.x * chunks;
-  out += blockIdx.x;
   __shared__ double part[1024];
-  __shared__ double red[32];
   const uint64_t per = (chunks + 1023) / 1024;
   const uint64_t b = threadIdx.x * per;
   const uint64_t e = min(chunks, b + per);
   double local = 0.0;
   for (uint64_t c = b; c < e; ++c) local += sums[c];
   part[threadIdx.x] = local;
-  const double total = block_sum<1024>(local, red);
-  __shared__ double s_total, s_scale;
+  __syncthreads();
   if (threadIdx.x == 0) {
-    s_total = total;
-    s_scale = (fabs(total - 1.0) > 1e-12 && total != 0.0) ? 1.0 / total : 1.0;
-    // exclusive scan of the per-thread partials (1024 adds, sequential, deterministic)
     double run = 0.0;
     for (int k = 0; k < 1024; ++k) {
       const double v = part[k];
       part[k] = run;
       run += v;
     }
-    out->total = total;
-    out->scale = s_scale;
-    out->status = (total == 0.0 || !isfinite(total)) ? 1 : 0;
   }
   __syncthreads();
-  const double scale = s_scale;
   double run = part[threadIdx.x];
   for (uint64_t c = b; c < e; ++c) {
-    prefix[c] = run * scale;
+    prefix[c] = run;
     run += sums[c];
   }
 }
 
-// pass C: one warp per shot.  In a batch, shot g belongs to state g / shots_per and
+// ---- integer form of the running sum inside one binade --------------------------
+constexpr int32_t kTfUsable = 4, kTfApplied = 8;  // ChunkTf::flags bits 2 and 3
+
+// effect of a run of additions on A (the running sum in ulps of one binade)
+struct Tf {
+  int64_t d0, d1;  // increments for an even / odd A
+  uint32_t p;      // bit 0: parity left for an even A, bit 1: for an odd A
+};
+
+__device__ __forceinline__ Tf tf_identity() { return Tf{0, 0, 2u}; }
+
+// t1 then t2
+__device__ __forceinline__ Tf tf_compose(const Tf& t1, const Tf& t2) {
+  const uint32_t q0 = t1.p & 1u, q1 = (t1.p >> 1) & 1u;
+  Tf r;
+  r.d0 = t1.d0 + (q0 ? t2.d1 : t2.d0);
+  r.d1 = t1.d1 + (q1 ? t2.d1 : t2.d0);
+  r.p = ((t2.p >> q0) & 1u) | (((t2.p >> q1) & 1u) << 1);
+  return r;
+}
+
+// the addition of p (>= 0) to a running sum in binade e, as an effect on A; *bad is
+// set when p alone is too large to keep the sum in the binade
+__device__ __forceinline__ Tf tf_of(double p, int e, bool* bad) {
+  if (!(p > 0.0)) return tf_identity();
+  const uint64_t bits = (uint64_t)__double_as_longlong(p);
+  const int E = (int)((bits >> 52) & 0x7ffu);
+  const uint64_t F = bits & ((1ULL << 52) - 1ULL);
+  const uint64_t m = E ? (F | (1ULL << 52)) : F;
+  const int q = E ? E - 1075 : -1074;  // p = m * 2^q
+  const int s = q + 52 - e;            // p / ulp = m * 2^s
+  uint64_t f;
+  int cmp;  // fraction of p / ulp against one half: -1 below, 0 equal, 1 above
+  if (s >= 0) {
+    if (s > 9) {  // p / ulp >= 2^62: the sum leaves the binade
+      *bad = true;
+      return tf_identity();
+    }
+    f = m << s;
+    cmp = -1;
+  } else {
+    const int t = -s;
+    if (t >= 64) {
+      f = 0;
+      cmp = -1;  // m < 2^53 < 2^63: below one half
+    } else {
+      f = m >> t;
+      const uint64_t rem = m & ((1ULL << t) - 1ULL);
+      const uint64_t half = 1ULL << (t - 1);
+      cmp = rem < half ? -1 : (rem == half ? 0 : 1);
+    }
+  }
+  Tf r;
+  if (cmp != 0) {
+    const int64_t d = (int64_t)f + (cmp > 0 ? 1 : 0);
+    r.d0 = r.d1 = d;
+    const uint32_t dp = (uint32_t)(d & 1);
+    r.p = dp | ((dp ^ 1u) << 1);
+  } else {  // half-way: to the even neighbour, which leaves A even
+    r.d0 = (int64_t)f + (int64_t)(f & 1ULL);
+    r.d1 = (int64_t)f + (int64_t)((f + 1ULL) & 1ULL);
+    r.p = 0u;
+  }
+  return r;
+}
+
+__device__ __forceinline__ Tf tf_shfl_up(const Tf& t, int o) {
+  Tf r;
+  r.d0 = __shfl_up_sync(0xffffffffu, t.d0, o);
+  r.d1 = __shfl_up_sync(0xffffffffu, t.d1, o);
+  r.p = __shfl_up_sync(0xffffffffu, t.p, o);
+  return r;
+}
+
+// inclusive in-order scan of the lanes' effects
+__device__ __forceinline__ Tf tf_warp_scan(Tf t, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const Tf u = tf_shfl_up(t, o);
+    if (lane >= o) t = tf_compose(u, t);
+  }
+  return t;
+}
+
+// binade exponent of a positive normal double, or -2000 otherwise
+__device__ __forceinline__ int binade(double s) {
+  const uint64_t bits = (uint64_t)__double_as_longlong(s);
+  const int E = (int)((bits >> 52) & 0x7ffu);
+  return (E == 0 || E == 0x7ff || (bits >> 63)) ? -2000 : E - 1023;
+}
+
+// S = A * 2^(e - 52) with A in [2^52, 2^53): an effect applied to S, exactly; false
+// when the result would leave the binade
+__device__ __forceinline__ bool tf_apply(const Tf& t, int e, double* s) {
+  const uint64_t bits = (uint64_t)__double_as_longlong(*s);
+  const uint64_t A = (bits & ((1ULL << 52) - 1ULL)) | (1ULL << 52);
+  const uint64_t An = A + (uint64_t)((A & 1ULL) ? t.d1 : t.d0);
+  if (An >= (1ULL << 53)) return false;
+  *s = __longlong_as_double((long long)(((uint64_t)(e + 1023) << 52) | (An - (1ULL << 52))));
+  return true;
+}
+
+// pass C: per chunk, the binade its running sum stays in (from the approximate
+// running sums, with a margin of 2^-18 relative, far above the summation error of at
+// most 2^32 * 2^-53 relative) and its effect there
+template <typename Src>
+__global__ void __launch_bounds__(kThreadsA) k_chunk_tf(Src src, uint64_t len_per,
+                                                        uint64_t chunks_per, uint64_t chunks,
+                                                        const double* prefix,
+                                                        const SampleScalars* sc,
+                                                        bool scaled_pass, ChunkTf* out) {
+  __shared__ Tf wtf[kThreadsA / 32];
+  __shared__ int s_e, s_bad;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr double kMargin = 0x1p-18;
+  for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+    const uint64_t st = c / chunks_per;
+    if (scaled_pass && !sc[st].scaled) continue;
+    const double scale = scaled_pass ? sc[st].scale : 1.0;
+    const uint64_t cl = c - st * chunks_per;
+    if (threadIdx.x == 0) {
+      // clean: the whole chunk inside [2^e, 2^(e+1)) with the margin on both ends (the
+      // last chunk, whose end is the total, is always added element by element)
+      bool clean = cl + 1 < chunks_per;
+      int e = -2000;
+      if (clean) {
+        const double a = prefix[c], b = prefix[c + 1];
+        e = binade(a * (1.0 - kMargin));
+        clean = e > -1000 && binade(a) == e && binade(b * (1.0 + kMargin)) == e;
+      }
+      s_e = clean ? e : -2000;
+      s_bad = 0;
+    }
+    __syncthreads();
+    const int e = s_e;
+    if (e < -1000) {
+      if (threadIdx.x == 0) out[c] = ChunkTf{0, 0, 0, 0};
+      __syncthreads();
+      continue;
+    }
+    const uint64_t b0 = cl * kChunk + (uint64_t)threadIdx.x * (kChunk / kThreadsA);
+    const uint64_t off = st * len_per;
+    bool bad = false;
+    Tf t = tf_identity();
+    for (int k = 0; k < kChunk / kThreadsA; ++k) {
+      const uint64_t i = b0 + k;
+      if (i >= len_per) break;
+      double pv = src(off + i);
+      if (scaled_pass) pv = __dmul_rn(pv, scale);
+      t = tf_compose(t, tf_of(pv, e, &bad));
+    }
+    t = tf_warp_scan(t, lane);
+    const bool any_bad = __any_sync(0xffffffffu, bad);
+    if (lane == 31) {
+      wtf[warp] = t;
+      if (any_bad) s_bad = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      Tf r = tf_identity();
+      for (int w = 0; w < kThreadsA / 32; ++w) r = tf_compose(r, wtf[w]);
+      out[c] = ChunkTf{r.d0, r.d1, (int32_t)(r.p & 3u) | (s_bad ? 0 : kTfUsable), e};
+    }
+    __syncthreads();
+  }
+}
+
+// pass D (one CTA per state): the exact running sum before each chunk, in chunk
+// order from S = 0; the exact total, the rescaling decision and the status.  On the
+// rescaled pass, only the states the reference rescales.  Thread 0 steps through the
+// chunks; the whole CTA joins in only to stage a chunk that is added element by
+// element.
+template <typename Src>
+__global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per,
+                                                       uint64_t chunks_per, ChunkTf* tfs,
+                                                       double* starts, SampleScalars* sc,
+                                                       bool scaled_pass) {
+  const uint64_t st = blockIdx.x;
+  if (scaled_pass && !sc[st].scaled) return;
+  const double scale = scaled_pass ? sc[st].scale : 1.0;
+  tfs += st * chunks_per;
+  starts += st * chunks_per;
+  const uint64_t off = st * len_per;
+  __shared__ ChunkTf blk[1024];
+  __shared__ double elems[kChunk];
+  __shared__ uint32_t s_next;
+  double S = 0.0;  // thread 0's running sum
+  for (uint64_t c0 = 0; c0 < chunks_per; c0 += 1024) {
+    const uint32_t n_blk = (uint32_t)min((uint64_t)1024, chunks_per - c0);
+    __syncthreads();
+    if (threadIdx.x < n_blk) blk[threadIdx.x] = tfs[c0 + threadIdx.x];
+    __syncthreads();
+    for (uint32_t k = 0; k < n_blk;) {
+      if (threadIdx.x == 0) {
+        // apply chunk records while they keep the sum in their binade
+        uint32_t q = k;
+        for (; q < n_blk; ++q) {
+          ChunkTf& r = blk[q];
+          if (!(r.flags & kTfUsable) || binade(S) != r.e) break;
+          const Tf t{r.d0, r.d1, (uint32_t)(r.flags & 3)};
+          double Sn = S;
+          if (!tf_apply(t, r.e, &Sn)) break;
+          starts[c0 + q] = S;
+          S = Sn;
+          r.flags |= kTfApplied;
+        }
+        s_next = q;
+      }
+      __syncthreads();
+      k = s_next;
+      if (k >= n_blk) break;
+      // chunk k: element by element, exact FP64 adds in the reference's order
+      const uint64_t b = (c0 + k) * kChunk;
+      for (int q = threadIdx.x; q < kChunk; q += blockDim.x) {
+        const uint64_t i = b + q;
+        double pv = i < len_per ? src(off + i) : 0.0;
+        if (scaled_pass) pv = __dmul_rn(pv, scale);
+        elems[q] = pv;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        starts[c0 + k] = S;
+        blk[k].flags &= ~kTfApplied;
+        const uint64_t lim = min((uint64_t)kChunk, len_per - b);
+        for (uint64_t q = 0; q < lim; ++q) S = __dadd_rn(S, elems[q]);
+      }
+      __syncthreads();
+      ++k;
+    }
+    __syncthreads();
+    if (threadIdx.x < n_blk) tfs[c0 + threadIdx.x].flags = blk[threadIdx.x].flags;
+  }
+  if (threadIdx.x == 0 && !scaled_pass) {
+    // normalize (StatevectorEngine.java:298-312): a zero sum is an error; rescale by
+    // 1.0 / sum when |sum - 1| > 1e-12
+    sc[st].total = S;
+    const bool zero = !(S > 0.0) || !isfinite(S);
+    sc[st].status = zero ? 1 : 0;
+    const bool rescale = !zero && fabs(S - 1.0) > 1e-12;
+    sc[st].scaled = rescale ? 1 : 0;
+    sc[st].scale = rescale ? __ddiv_rn(1.0, S) : 1.0;
+  }
+}
+
+// pass E: one warp per shot.  In a batch, shot g belongs to state g / shots_per and
 // draws the (g % shots_per)-th uniform of SplittableRandom(seed + state).
 template <typename Src>
 __global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
-                                                      const double* prefix_all, uint64_t chunks,
+                                                      const double* starts_all,
+                                                      const ChunkTf* tfs_all, uint64_t chunks,
                                                       const SampleScalars* sc,
                                                       const double* uniforms, uint64_t seed,
                                                       int64_t shots_per, int64_t shots_total,
@@ -128,19 +385,24 @@ __global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
     const int64_t stn = g / shots_per;
     const int64_t k = g - stn * shots_per;
     const uint64_t off = (uint64_t)stn * len;
-    auto src = [&](uint64_t i) { return src_all(off + i); };
-    const double* prefix = prefix_all + (uint64_t)stn * chunks;
+    const double* starts = starts_all + (uint64_t)stn * chunks;
+    const ChunkTf* tfs = tfs_all + (uint64_t)stn * chunks;
+    const bool scaled = sc[stn].scaled != 0;
     const double scale = sc[stn].scale;
+    auto prob = [&](uint64_t i) {
+      const double v = src_all(off + i);
+      return scaled ? __dmul_rn(v, scale) : v;
+    };
     const double u = uniforms ? uniforms[g] : splitmix_double(seed + (uint64_t)stn, (uint64_t)k);
     if (u >= 1.0) {
       if (lane == 0) out[g] = (int32_t)(len - 1);
       continue;
     }
-    // last chunk whose prefix is < u (prefix[0] == 0)
+    // last chunk whose exact start is < u (starts[0] == 0)
     int64_t lo = 0, hi = (int64_t)chunks - 1, j = 0;
     while (lo <= hi) {
       const int64_t mid = (lo + hi) >> 1;
-      if (prefix[mid] < u) {
+      if (starts[mid] < u) {
         j = mid;
         lo = mid + 1;
       } else {
@@ -148,39 +410,57 @@ __global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
       }
     }
     const uint64_t b = (uint64_t)j * kChunk;
-    constexpr int per = kChunk / 32;
-    const uint64_t lb = b + (uint64_t)lane * per;
-    double lsum = 0.0;
-    for (int q = 0; q < per; ++q) {
-      const uint64_t i = lb + q;
-      if (i < len) lsum += src(i) * scale;
-    }
-    // exclusive warp scan of lane sums
-    double incl = lsum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const double y = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= o) incl += y;
-    }
-    double run = prefix[j] + (incl - lsum);
+    const ChunkTf rec = tfs[j];
     uint64_t found = ~0ULL;
-    for (int q = 0; q < per; ++q) {
-      const uint64_t i = lb + q;
-      if (i >= len) break;
-      run += src(i) * scale;
-      if (i == len - 1 || run >= u) {  // the last entry is 1.0
-        found = i;
-        break;
+    if (rec.flags & kTfApplied) {
+      // the chunk's sum stays in binade rec.e: each lane's start from the lanes'
+      // effects, then exact FP64 adds inside the lane
+      constexpr int per = kChunk / 32;
+      const uint64_t lb = b + (uint64_t)lane * per;
+      bool bad = false;
+      Tf t = tf_identity();
+      for (int q = 0; q < per; ++q) {
+        const uint64_t i = lb + q;
+        if (i >= len) break;
+        t = tf_compose(t, tf_of(prob(i), rec.e, &bad));
       }
-    }
+      const Tf incl = tf_warp_scan(t, lane);
+      Tf excl = tf_shfl_up(incl, 1);
+      if (lane == 0) excl = tf_identity();
+      double run = starts[j];
+      tf_apply(excl, rec.e, &run);
+      for (int q = 0; q < per; ++q) {
+        const uint64_t i = lb + q;
+        if (i >= len) break;
+        run = __dadd_rn(run, prob(i));
+        if (i == len - 1 || run >= u) {  // the last entry is 1.0
+          found = i;
+          break;
+        }
+      }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const uint64_t y = __shfl_xor_sync(0xffffffffu, found, o);
-      found = y < found ? y : found;
+      for (int o = 16; o > 0; o >>= 1) {
+        const uint64_t y = __shfl_xor_sync(0xffffffffu, found, o);
+        found = y < found ? y : found;
+      }
+    } else if (lane == 0) {
+      // element by element from the chunk's exact start
+      double run = starts[j];
+      const uint64_t lim = min((uint64_t)kChunk, len - b);
+      for (uint64_t q = 0; q < lim; ++q) {
+        const uint64_t i = b + q;
+        run = __dadd_rn(run, prob(i));
+        if (i == len - 1 || run >= u) {
+          found = i;
+          break;
+        }
+      }
     }
     if (lane == 0) {
       uint64_t r = found;
-      if (r == ~0ULL) r = min(len - 1, b + kChunk);  // rounding gap: first entry of the next chunk
+      // not reached inside the chunk (the running sum at the chunk's end is >= u by
+      // the search, so only a last-chunk tail below u): the last entry, forced to 1.0
+      if (r == ~0ULL) r = min(len - 1, b + kChunk);
       out[g] = (int32_t)r;
     }
   }
@@ -271,14 +551,28 @@ cudaError_t sample_src(Src src, uint64_t len, int64_t batch, const SampleArgs& a
                        cudaStream_t s) {
   const uint64_t chunks = (len + kChunk - 1) / kChunk;
   const uint64_t all_chunks = chunks * (uint64_t)batch;
-  k_chunk_sums<Src><<<grid_cap(all_chunks * kThreadsA, kThreadsA, a.sm_count), kThreadsA, 0, s>>>(
-      src, len, chunks, a.chunk_sums, all_chunks);
-  k_chunk_scan<<<(unsigned)batch, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix, a.scalars);
+  const int grid_chunks = grid_cap(all_chunks * kThreadsA, kThreadsA, a.sm_count);
+  cudaError_t e = cudaMemsetAsync(a.scalars, 0, sizeof(SampleScalars) * (size_t)batch, s);
+  if (e != cudaSuccess) return e;
+  // the running sum of the probabilities, then (decided on the device, per state) of
+  // the rescaled probabilities when the reference rescales
+  for (int pass = 0; pass < 2; ++pass) {
+    const SampleScalars* gate = pass ? a.scalars : nullptr;
+    k_chunk_sums<Src><<<grid_chunks, kThreadsA, 0, s>>>(src, len, chunks, a.chunk_sums,
+                                                        all_chunks, gate);
+    k_prefix_approx<<<(unsigned)batch, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix, gate);
+    k_chunk_tf<Src><<<grid_chunks, kThreadsA, 0, s>>>(src, len, chunks, all_chunks,
+                                                      a.chunk_prefix, a.scalars, pass == 1,
+                                                      a.chunk_tf);
+    k_exact_starts<Src><<<(unsigned)batch, 1024, 0, s>>>(src, len, chunks, a.chunk_tf,
+                                                         a.chunk_start, a.scalars, pass == 1);
+  }
   if (a.shots > 0) {
     const int64_t total = a.shots * batch;
     const int blocks = grid_cap((uint64_t)total * 32, 256, a.sm_count);
-    k_sample_shots<Src><<<blocks, 256, 0, s>>>(src, len, a.chunk_prefix, chunks, a.scalars,
-                                               a.uniforms, a.seed, a.shots, total, a.outcomes);
+    k_sample_shots<Src><<<blocks, 256, 0, s>>>(src, len, a.chunk_start, a.chunk_tf, chunks,
+                                               a.scalars, a.uniforms, a.seed, a.shots, total,
+                                               a.outcomes);
   }
   return cudaGetLastError();
 }

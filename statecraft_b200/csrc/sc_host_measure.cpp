@@ -59,7 +59,9 @@ int Ctx::sample(const int32_t* qubits, int32_t m, int64_t shots, uint64_t seed,
   }
   const uint64_t chunks = sample_chunks(len);
   const size_t off_prefix = sizeof(double) * chunks;
-  const size_t off_scalars = 2 * off_prefix;
+  const size_t off_start = 2 * off_prefix;
+  const size_t off_tf = 3 * off_prefix;
+  const size_t off_scalars = off_tf + sizeof(ChunkTf) * chunks;
   const size_t off_uniforms = off_scalars + 64;
   const size_t off_outcomes = off_uniforms + (uniforms ? sizeof(double) * (size_t)shots : 0);
   const size_t total = off_outcomes + sizeof(int32_t) * (size_t)shots + 16;
@@ -68,6 +70,8 @@ int Ctx::sample(const int32_t* qubits, int32_t m, int64_t shots, uint64_t seed,
   SampleArgs a;
   a.chunk_sums = reinterpret_cast<double*>(base);
   a.chunk_prefix = reinterpret_cast<double*>(base + off_prefix);
+  a.chunk_start = reinterpret_cast<double*>(base + off_start);
+  a.chunk_tf = reinterpret_cast<ChunkTf*>(base + off_tf);
   a.scalars = reinterpret_cast<SampleScalars*>(base + off_scalars);
   a.uniforms = uniforms ? reinterpret_cast<const double*>(base + off_uniforms) : nullptr;
   a.seed = seed;

@@ -9,16 +9,31 @@ namespace sc {
 constexpr int kSampleChunk = 2048;  // probabilities per chunk of the two-level prefix sum
 
 struct SampleScalars {
-  double total;  // sum of the probabilities
+  double total;  // the reference's left-to-right sum of the probabilities (exact)
   double scale;  // 1/total when |total - 1| > 1e-12, else 1
   int32_t status;  // 1: zero or non-finite total
-  int32_t pad;
+  int32_t scaled;  // 1: the probabilities are rescaled by `scale` before the running sum
+};
+
+// Per-chunk record of the exact running sum (k_measure.cu): the effect of the chunk's
+// additions on a running sum that stays in one binade [2^e, 2^(e+1)), as integer
+// increments in units of that binade's ulp for an even (d0) and an odd (d1) running
+// sum, and the parity it leaves (flags bit 0: for an even sum, bit 1: for an odd
+// one); flags bit 2: usable (the chunk lies in one binade and the record was
+// computed); bit 3: set by the exact pass when the record was applied (else the
+// chunk was added element by element).
+struct ChunkTf {
+  int64_t d0, d1;
+  int32_t flags;
+  int32_t e;
 };
 
 struct SampleArgs {
-  double* chunk_sums;    // device, sample_chunks(len) doubles
-  double* chunk_prefix;  // device, sample_chunks(len) doubles
-  SampleScalars* scalars;  // device
+  double* chunk_sums;    // device, sample_chunks(len) doubles per state
+  double* chunk_prefix;  // device, the same: approximate running sums before each chunk
+  double* chunk_start;   // device, the same: exact running sums before each chunk
+  ChunkTf* chunk_tf;     // device, sample_chunks(len) records per state
+  SampleScalars* scalars;  // device, one per state
   const double* uniforms;  // device or nullptr (then SplitMix64(seed))
   uint64_t seed;
   int64_t shots;         // 0: only the prefix sums

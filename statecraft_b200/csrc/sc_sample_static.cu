@@ -9,11 +9,12 @@
 // memory and want outcomes written into their own device buffer.
 //
 // sc_sample_static samples every qubit of such a state (outcome = basis index, the
-// countsAll convention) with the same kernels as sc_sample.  Its only scratch, the
-// chunk sums, chunk prefixes and scalars of the two-level FP64 prefix sum, lives in
-// the file-scope array below: room for states of up to kStaticMaxAmps = 2^30
-// amplitudes (30 qubits), about 8 MiB that every GPU which loads this library holds
-// until the process exits.  Larger states are rejected with SC_EINVAL.
+// countsAll convention) with the same kernels as sc_sample.  Its only scratch -- the
+// per-chunk sums, approximate and exact running sums and records of the running sum,
+// and the scalars -- lives in the file-scope array below: room for states of up to
+// kStaticMaxAmps = 2^30 amplitudes (30 qubits), about 24 MiB that every GPU which
+// loads this library holds until the process exits.  Larger states are rejected with
+// SC_EINVAL.
 //
 // The array's name is a host-side stand-in in host code, so its device address is
 // looked up with cudaGetSymbolAddress once per device, with that device current,
@@ -37,8 +38,11 @@ namespace {
 
 constexpr uint64_t kStaticMaxAmps = 1ULL << 30;
 constexpr uint64_t kStaticChunks = kStaticMaxAmps / kSampleChunk;
-// layout: chunk sums [kStaticChunks] | chunk prefixes [kStaticChunks] | scalars
-constexpr uint64_t kStaticDoubles = 2 * kStaticChunks + 8;
+// layout: chunk sums | approximate running sums | exact running sums [kStaticChunks
+// doubles each] | chunk records [kStaticChunks ChunkTf] | scalars
+static_assert(sizeof(ChunkTf) % sizeof(double) == 0, "records pack into doubles");
+constexpr uint64_t kTfDoubles = sizeof(ChunkTf) / sizeof(double);
+constexpr uint64_t kStaticDoubles = (3 + kTfDoubles) * kStaticChunks + 8;
 static_assert(sizeof(SampleScalars) <= 8 * sizeof(double), "scalars must fit the tail");
 
 static __device__ __align__(256) double g_sample_scratch[kStaticDoubles];
@@ -90,7 +94,9 @@ extern "C" int32_t sc_sample_static(const void* d_state, int32_t n_qubits, int32
   SampleArgs a;
   a.chunk_sums = scratch;
   a.chunk_prefix = scratch + kStaticChunks;
-  a.scalars = reinterpret_cast<SampleScalars*>(scratch + 2 * kStaticChunks);
+  a.chunk_start = scratch + 2 * kStaticChunks;
+  a.chunk_tf = reinterpret_cast<ChunkTf*>(scratch + 3 * kStaticChunks);
+  a.scalars = reinterpret_cast<SampleScalars*>(scratch + (3 + kTfDoubles) * kStaticChunks);
   a.uniforms = d_uniforms;
   a.seed = seed;
   a.shots = shots;

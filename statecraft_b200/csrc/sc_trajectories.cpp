@@ -163,7 +163,9 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
   const size_t off_codes = 0;
   const size_t off_sums = (paulis.size() + 255) & ~(size_t)255;
   const size_t off_prefix = off_sums + sizeof(double) * chunks * (size_t)n_traj;
-  const size_t off_scalars = off_prefix + sizeof(double) * chunks * (size_t)n_traj;
+  const size_t off_start = off_prefix + sizeof(double) * chunks * (size_t)n_traj;
+  const size_t off_tf = off_start + sizeof(double) * chunks * (size_t)n_traj;
+  const size_t off_scalars = off_tf + sizeof(ChunkTf) * chunks * (size_t)n_traj;
   const size_t off_out = off_scalars + sizeof(SampleScalars) * (size_t)n_traj;
   const size_t aux_bytes = off_out + sizeof(int32_t) * (size_t)std::max<int64_t>(1, shots * n_traj);
   if ((rc = c->reserve(c->buf_traj_states, state_bytes, "trajectory states")) != SC_OK) return rc;
@@ -194,6 +196,8 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
     SampleArgs a;
     a.chunk_sums = reinterpret_cast<double*>(aux + off_sums);
     a.chunk_prefix = reinterpret_cast<double*>(aux + off_prefix);
+    a.chunk_start = reinterpret_cast<double*>(aux + off_start);
+    a.chunk_tf = reinterpret_cast<ChunkTf*>(aux + off_tf);
     a.scalars = reinterpret_cast<SampleScalars*>(aux + off_scalars);
     a.uniforms = nullptr;
     a.seed = measure_seed;

@@ -156,6 +156,42 @@ def test_sampling_bit_exact_on_shared_uniforms(n, m_qubits, fused):
     np.testing.assert_array_equal(ctx.sample(qubits, shots, 1234), gpu)
 
 
+@pytest.mark.parametrize("scale", [1.0, 1.5, 0.25 + 1e-9])
+def test_sampling_reproduces_the_reference_running_sum(scale, fused):
+    # the running sum of 2^16 probabilities, with the reference's rescaling when the
+    # total is off by more than 1e-12 (scale != 1): outcomes identical on shared
+    # uniforms, including draws placed exactly on CDF entries and half-way ties
+    n = 16
+    init = RCirc.random_state(n, 21) * math.sqrt(scale)
+    ctx = fused.context()
+    ctx.run_ops(n, *serialize_circuit(Q.QuantumCircuit(n)), init)
+    cdf = O.cumulative(O.probabilities(init, n, list(range(n))))
+    rng = np.random.default_rng(3)
+    u = np.concatenate([rng.random(3000), cdf[rng.integers(0, cdf.size - 1, 500)],
+                        np.nextafter(cdf[rng.integers(0, cdf.size - 1, 500)], 0)])
+    got = ctx.sample(list(range(n)), u.size, None, u)
+    want = O.sample(init, n, list(range(n)), u.size, 0, u)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_sampling_dyadic_probabilities_with_ties(fused):
+    # probabilities that are sums of few powers of two make the running sum hit
+    # half-way cases of round-to-nearest-even; a state of 2^18 such entries
+    n = 18
+    rng = np.random.default_rng(8)
+    p = rng.choice([0.0, 2.0 ** -18, 2.0 ** -20, 3 * 2.0 ** -21, 2.0 ** -40], size=1 << n)
+    p[-1] += 1.0 - p.sum()
+    init = np.zeros(2 << n)
+    init[0::2] = np.sqrt(np.maximum(p, 0.0))
+    ctx = fused.context()
+    ctx.run_ops(n, *serialize_circuit(Q.QuantumCircuit(n)), init)
+    cdf = O.cumulative(O.probabilities(init, n, list(range(n))))
+    u = np.concatenate([rng.random(4000), cdf[rng.integers(0, cdf.size - 1, 1000)]])
+    got = ctx.sample(list(range(n)), u.size, None, u)
+    want = O.sample(init, n, list(range(n)), u.size, 0, u)
+    np.testing.assert_array_equal(got, want)
+
+
 def test_tie_rule_and_last_entry(fused):
     # state with exact probabilities 1/4, 0, 1/4, 1/2 on 2 qubits
     init = np.array([0.5, 0, 0, 0, 0.5, 0, math.sqrt(0.5), 0])
