@@ -48,7 +48,8 @@ def parse_args(argv=None):
     ap.add_argument("--sweep-budget", type=int, default=0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", choices=["statevector", "c1", "qaoa", "adjoint", "trajectories"],
+    ap.add_argument("--workload", choices=["statevector", "c1", "qaoa", "adjoint", "trajectories",
+                                           "blocks"],
                     default="statevector",
                     help="statevector: the headline line; c1: the 20-qubit plain drop-in; "
                          "the others time the batched QAOA, adjoint-gradient and "
@@ -472,6 +473,59 @@ def run_c1(args) -> dict:
             "clocks": clk.summary()}
 
 
+def run_blocks(args) -> dict:
+    """Dense tensor-core blocks against the sweep path on a circuit made for them:
+    28 qubits, 60 rounds of 12 gates inside random 5-qubit windows (dense random
+    two-qubit unitaries, CNOTs, U3, controlled phases; a 27-control MCZ every third
+    round).  Both timings are sc_run on the device with the state resident."""
+    import torch
+
+    from statecraft_b200 import workloads as W
+    from statecraft_b200.engine import B200Config, NativeContext, serialize_circuit
+
+    n = 28
+    c = W.dense_window_circuit(n, 60, seed=2828)
+    ops, n_ops = serialize_circuit(c)
+    updates = W.amp_updates(c)
+    out = {}
+    for name, thr in (("sweeps", "0"), ("blocks", "1"), ("blocks_cost64", "64")):
+        os.environ["STATECRAFT_B200_DENSE_BLOCKS"] = thr
+        ctx = NativeContext(B200Config(timing=True))
+        for _ in range(max(args.warmup, 1)):
+            ctx.run_ops(n, ops, n_ops)
+        ctx.reset_kernel_stats()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ctx.run_ops(n, ops, n_ops)
+        torch.cuda.synchronize()
+        sec = (time.perf_counter() - t0) / args.steps
+        stats = {k: v for k, v in ctx.kernel_stats().items() if v["launches"]}
+        out[name] = {"s_per_run": sec, "plan": ctx.plan_stats(), "kernel_stats": stats}
+        ctx.close()
+    os.environ.pop("STATECRAFT_B200_DENSE_BLOCKS", None)
+    blk = out["blocks"]["kernel_stats"].get("block", {"launches": 0, "ms": 0.0, "bytes": 0.0})
+    peak = measured_peaks().get("hbm_gbs") or 6650.0
+    gbs = blk["bytes"] / (blk["ms"] / 1e3) / 1e9 if blk["ms"] else None
+    return {"metric": "amp-updates/s (28q dense 5-qubit-window circuit, tensor-core blocks vs sweeps)",
+            "value": updates / out["blocks"]["s_per_run"], "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * out["blocks"]["s_per_run"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "dense 5-qubit windows", "qubits": n, "rounds": 60,
+                       "seed": 2828, "amp_updates_per_step": updates},
+            "sweeps_only": {"value": updates / out["sweeps"]["s_per_run"],
+                            "ms_per_step": 1e3 * out["sweeps"]["s_per_run"],
+                            "plan": out["sweeps"]["plan"]},
+            "blocks": {"plan": out["blocks"]["plan"], "kernel_stats": out["blocks"]["kernel_stats"],
+                       "note": "every run of gates on <= 5 qubits (at least 3) as a dense block"},
+            "blocks_cost64": {"value": updates / out["blocks_cost64"]["s_per_run"],
+                              "ms_per_step": 1e3 * out["blocks_cost64"]["s_per_run"],
+                              "plan": out["blocks_cost64"]["plan"]},
+            "roofline_block_kernel": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",
+                                      "frac": (gbs / peak) if gbs else None}}
+
+
 # ---------------------------------------------------------------------------
 # the B200 engine
 # ---------------------------------------------------------------------------
@@ -485,7 +539,7 @@ def main(argv=None) -> int:
         return 0
     if args.workload != "statevector":
         fn = {"c1": run_c1, "qaoa": run_qaoa, "adjoint": run_adjoint,
-              "trajectories": run_trajectories_bench}[args.workload]
+              "trajectories": run_trajectories_bench, "blocks": run_blocks}[args.workload]
         print(json.dumps(fn(args)), flush=True)
         return 0
 

@@ -293,9 +293,11 @@ __global__ void __launch_bounds__(kThreadsA) k_chunk_tf(Src src, uint64_t len_pe
 
 // pass D (one CTA per state): the exact running sum before each chunk, in chunk
 // order from S = 0; the exact total, the rescaling decision and the status.  On the
-// rescaled pass, only the states the reference rescales.  Thread 0 steps through the
-// chunks; the whole CTA joins in only to stage a chunk that is added element by
-// element.
+// rescaled pass, only the states the reference rescales.  Chunks go in blocks of
+// 1024: a block whose records all lie in the binade of the running sum is one
+// in-order scan of their effects (each thread then applies its exclusive prefix to
+// the block's start); any other block is walked by thread 0, record by record, and
+// the whole CTA joins in to stage each chunk that is added element by element.
 template <typename Src>
 __global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per,
                                                        uint64_t chunks_per, ChunkTf* tfs,
@@ -307,15 +309,58 @@ __global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per
   tfs += st * chunks_per;
   starts += st * chunks_per;
   const uint64_t off = st * len_per;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   __shared__ ChunkTf blk[1024];
   __shared__ double elems[kChunk];
+  __shared__ Tf wsum[32];
   __shared__ uint32_t s_next;
-  double S = 0.0;  // thread 0's running sum
+  __shared__ int s_all_ok;
+  __shared__ double s_S;  // the running sum at the start of the current block
+  if (threadIdx.x == 0) s_S = 0.0;
   for (uint64_t c0 = 0; c0 < chunks_per; c0 += 1024) {
     const uint32_t n_blk = (uint32_t)min((uint64_t)1024, chunks_per - c0);
     __syncthreads();
+    if (threadIdx.x == 0) s_all_ok = 1;
     if (threadIdx.x < n_blk) blk[threadIdx.x] = tfs[c0 + threadIdx.x];
     __syncthreads();
+    // the scan path: every record usable and in the binade of the running sum
+    const double S0 = s_S;
+    const int e0 = binade(S0);
+    Tf t = tf_identity();
+    if (threadIdx.x < n_blk) {
+      const ChunkTf& r = blk[threadIdx.x];
+      if (!(r.flags & kTfUsable) || r.e != e0) s_all_ok = 0;
+      t = Tf{r.d0, r.d1, (uint32_t)(r.flags & 3)};
+    }
+    __syncthreads();
+    if (s_all_ok && e0 > -1000) {
+      const Tf incl = tf_warp_scan(t, lane);
+      if (lane == 31) wsum[warp] = incl;
+      __syncthreads();
+      if (warp == 0) {
+        const Tf w = tf_warp_scan(lane < (int)(blockDim.x >> 5) ? wsum[lane] : tf_identity(), lane);
+        wsum[lane] = w;  // inclusive over warps
+      }
+      __syncthreads();
+      Tf excl = tf_shfl_up(incl, 1);
+      if (lane == 0) excl = tf_identity();
+      if (warp > 0) excl = tf_compose(wsum[warp - 1], excl);
+      // the whole block stays in the binade when its total does (increments are >= 0)
+      double end = S0;
+      const bool fits = tf_apply(wsum[(blockDim.x >> 5) - 1], e0, &end);
+      if (fits) {
+        if (threadIdx.x < n_blk) {
+          double sv = S0;
+          tf_apply(excl, e0, &sv);
+          starts[c0 + threadIdx.x] = sv;
+          tfs[c0 + threadIdx.x].flags = blk[threadIdx.x].flags | kTfApplied;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_S = end;
+        continue;
+      }
+    }
+    double S = S0;  // thread 0's running sum on the walk path
     for (uint32_t k = 0; k < n_blk;) {
       if (threadIdx.x == 0) {
         // apply chunk records while they keep the sum in their binade
@@ -323,9 +368,9 @@ __global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per
         for (; q < n_blk; ++q) {
           ChunkTf& r = blk[q];
           if (!(r.flags & kTfUsable) || binade(S) != r.e) break;
-          const Tf t{r.d0, r.d1, (uint32_t)(r.flags & 3)};
+          const Tf tq{r.d0, r.d1, (uint32_t)(r.flags & 3)};
           double Sn = S;
-          if (!tf_apply(t, r.e, &Sn)) break;
+          if (!tf_apply(tq, r.e, &Sn)) break;
           starts[c0 + q] = S;
           S = Sn;
           r.flags |= kTfApplied;
@@ -355,10 +400,13 @@ __global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per
     }
     __syncthreads();
     if (threadIdx.x < n_blk) tfs[c0 + threadIdx.x].flags = blk[threadIdx.x].flags;
+    if (threadIdx.x == 0) s_S = S;
   }
+  __syncthreads();
   if (threadIdx.x == 0 && !scaled_pass) {
     // normalize (StatevectorEngine.java:298-312): a zero sum is an error; rescale by
     // 1.0 / sum when |sum - 1| > 1e-12
+    const double S = s_S;
     sc[st].total = S;
     const bool zero = !(S > 0.0) || !isfinite(S);
     sc[st].status = zero ? 1 : 0;

@@ -466,6 +466,13 @@ __device__ __forceinline__ void prex(typename Amp<R>::type (&v)[1 << NR], uint32
   }
 }
 
+// diagonal over the register bits as a table: register j times entry j
+template <typename R, int NR>
+__device__ __forceinline__ void dtab(typename Amp<R>::type (&v)[1 << NR], const R* m) {
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) v[j] = cmul(m[2 * j], m[2 * j + 1], v[j]);
+}
+
 // switch cases for the dispatch code (sw_code): one jump per gate into code that
 // is specialised on its register bits
 #define SC_CASE_1(K, A, F) \
@@ -535,59 +542,14 @@ __host__ __device__ __forceinline__ uint32_t tile_base(uint32_t t, const P& p) {
   return base;
 }
 
-// End of a stage.  A stage before the last writes its registers to their slots in
-// the next stage's layout (folded permutation and slot folds applied); the last
-// stage applies the sweep's scalar and stores the tile to global memory.  Each
-// branch consumes the registers, so none of them is live past it.
-template <typename R, int NR>
-__device__ __forceinline__ void stage_exit(const typename Amp<R>::type (&v)[1 << NR], bool last,
-                                           typename Amp<R>::type* cur, uint32_t wbase,
-                                           const SwStageTab& tab, const SlotFlips<NR>& fl,
-                                           typename Amp<R>::type* __restrict__ dst,
-                                           uint32_t gt_last, const SweepParams<R>& p) {
-  constexpr int NV = 1 << NR;
-  if (!last) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) cur[wbase ^ tab.wsoff[j] ^ fl[j]] = v[j];
-  } else if (p.has_scale) {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = cmul(p.scale_re, p.scale_im, v[j]);
-  } else {
-#pragma unroll
-    for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
-  }
-}
-
-// A stage whose only register record is one rotation-form record on the register
-// bits of M (M = 0: none): read, compute and exit as one piece of straight-line code.
-// The record's leading X, if any, is folded into tab.rd.
-template <typename R, int NR, int M>
-__device__ __forceinline__ void fast_stage(typename Amp<R>::type* cur, uint32_t rbase,
-                                           const SwStageTab& tab, const R* q, bool last,
-                                           uint32_t wbase, const SlotFlips<NR>& fl,
-                                           typename Amp<R>::type* __restrict__ dst,
-                                           uint32_t gt_last, const SweepParams<R>& p) {
-  constexpr int NV = 1 << NR;
-  typename Amp<R>::type v[NV];
-#pragma unroll
-  for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
-  if constexpr (M != 0) g1allq<R, NR, M>(v, q);
-  if (!last) __syncthreads();  // every read of `cur` in this stage is done
-  stage_exit<R, NR>(v, last, cur, wbase, tab, fl, dst, gt_last, p);
-}
-
 // Register caps.  complex128 NR = 3: 96 registers let five 128-thread CTAs share an
 // SM (measured a few percent faster than the uncapped 128).  complex128 NR = 4: 168
-// for the general kernel (three CTAs per SM); the kernel of sweeps whose stages are
-// all straight-line rotation stages needs fewer (four CTAs per SM at 128).
+// (three CTAs per SM, the limit the two 32 KB tile buffers set anyway).
 #ifndef SC_SWEEP_C128_NR3_REGS
 #define SC_SWEEP_C128_NR3_REGS 96
 #endif
 #ifndef SC_SWEEP_C128_NR4_REGS
 #define SC_SWEEP_C128_NR4_REGS 168
-#endif
-#ifndef SC_SWEEP_C128_NR4_FAST_REGS
-#define SC_SWEEP_C128_NR4_FAST_REGS 128
 #endif
 
 template <typename R, int NR>
@@ -595,12 +557,11 @@ constexpr int sweep_max_threads() {
   return NR >= 4 ? (sizeof(R) == 8 ? 256 : 512) : (NR == 3 ? 512 : 1024);
 }
 
-template <typename R, int NR, bool kFast>
+template <typename R, int NR>
 constexpr int sweep_max_regs() {
-  return NR == 3 && sizeof(R) == 8 ? SC_SWEEP_C128_NR3_REGS
-         : NR == 4 && sizeof(R) == 8
-             ? (kFast ? SC_SWEEP_C128_NR4_FAST_REGS : SC_SWEEP_C128_NR4_REGS)
-             : std::min(255, 65536 / sweep_max_threads<R, NR>());
+  return NR == 3 && sizeof(R) == 8   ? SC_SWEEP_C128_NR3_REGS
+         : NR == 4 && sizeof(R) == 8 ? SC_SWEEP_C128_NR4_REGS
+                                     : std::min(255, 65536 / sweep_max_threads<R, NR>());
 }
 
 constexpr long long kWaitLimitCycles = 2000000000LL;  // ~1 s at 2 GHz
@@ -617,13 +578,15 @@ __host__ __device__ constexpr size_t sweep_smem_bytes(int T) {
 // one buffer, tile i + grid arrives in the other -- as one bulk tensor copy (TMA)
 // issued by thread 0 and completing on that buffer's mbarrier when kTma (the tile is
 // a box of the state tensor), else as per-thread cp.async copies of each thread's
-// first-stage registers.  Results leave from the last stage as direct 128-/64-bit
-// stores.  kBatch: the sweep runs over p.batch states back to back and Pauli slots
-// read the trajectory's choices, staged in shared memory.  kFast: every stage is a
-// straight-line rotation stage (no record loop compiled in).
-template <typename R, int NR, bool kTma, bool kBatch, bool kFast>
+// first-stage registers.  The registers stay live from stage to stage (each stage
+// boundary: the previous stage's registers go to their slots in this stage's
+// layout, then this stage's registers are read), and results leave from the last
+// stage as direct 128-/64-bit stores.  kBatch: the sweep runs over p.batch states
+// back to back and Pauli slots read the trajectory's choices, staged in shared
+// memory.
+template <typename R, int NR, bool kTma, bool kBatch>
 __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
-    __maxnreg__((sweep_max_regs<R, NR, kFast>()))
+    __maxnreg__((sweep_max_regs<R, NR>()))
     k_sweep(typename Amp<R>::type* __restrict__ st, const __grid_constant__ SweepParams<R> p,
             int* __restrict__ err) {
   using A = typename Amp<R>::type;
@@ -728,90 +691,66 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
       }
     }
 
-    A* const dst = item_state(t) + base;
+    A v[NV];
+    {
+      // both copy paths leave the tile in `cur` in the linear layout
+      const SwStageTab& tab = p.tabs[0];
+#pragma unroll
+      for (int j = 0; j < NV; ++j) v[j] = cur[l0_first ^ tab.rd[j]];
+    }
+    uint32_t l0 = l0_first, psw0 = 0;
+    RegOff<NR> off;
+    SlotFlips<NR> sidx;
 #pragma unroll 1
     for (int s = 0; s < ns; ++s) {
       const SwStage& stg = p.stages[s];
       const SwStageTab& tab = p.tabs[s];
-      const bool last = s + 1 == ns;
-      const uint32_t l0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
-      // where this stage reads its registers and where it writes them for the next
-      const uint32_t rbase = (s == 0) ? l0_first : stage_swz<R>(l0, tab);
-      const uint32_t wbase = last ? 0u : stage_swz<R>(l0, p.tabs[s + 1]);
-      if (s > 0) __syncthreads();  // the previous stage's exit stores are visible
-      SlotFlips<NR> sidx;
+      const uint32_t nl0 = (s == 0) ? l0_first : stage_l0<NR>(tid, stg);
+      if (s > 0) {
+        __syncthreads();  // readers of the buffer are done
+        // the previous stage's exit slots: its folded permutation (wsoff) and
+        // slot folds (sidx) applied, in this stage's layout
+        const SwStageTab& ptab = p.tabs[s - 1];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) cur[psw0 ^ ptab.wsoff[j] ^ sidx[j]] = v[j];
+        __syncthreads();
+        const uint32_t sw0 = stage_swz<R>(nl0, tab);
+#pragma unroll
+        for (int j = 0; j < NV; ++j) v[j] = cur[sw0 ^ tab.rd[j]];
+      }
+      // this stage's exit slots are in the next stage's layout
+      psw0 = s + 1 < ns ? stage_swz<R>(nl0, p.tabs[s + 1]) : 0u;
       sidx.x0 = 0u;
 #pragma unroll
       for (int k = 0; k < NR; ++k) sidx.xc[k] = 0u;
-      const int prog = tab.prog;
-      if (kFast || prog != kProgGeneric) {
-        // A stage with one rotation record: its other records are slot folds, which
-        // only change where registers leave (integer work, decided first); the
-        // registers then live in straight-line code from the read to the exit.
-#pragma unroll 1
-        for (int gi = stg.g0; gi < stg.g1; ++gi) {
-          const SwGate& g = p.gates[gi];
-          if (g.kind != SK_XF && g.kind != SK_CXF) continue;
-          if (((uint64_t)base & g.gmask) != g.gmask) continue;
-          const uint32_t m = (l0 & g.lmask) == g.lmask ? (uint32_t)tab.xoff[g.a] : 0u;
-          if (g.kind == SK_XF) {
-            sidx.x0 ^= m;
-          } else {
+      l0 = nl0;
 #pragma unroll
-            for (int k = 0; k < NR; ++k)
-              if (g.b == k) sidx.xc[k] ^= m;
-          }
-        }
-        const R* q = p.pool + tab.qoff;
-        switch (prog) {
-#define SC_FAST_CASE(M)                                                                   \
-  case (M):                                                                               \
-    if constexpr (((M) >> NR) == 0)                                                       \
-      fast_stage<R, NR, (M)>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last, p);     \
-    break;
-          SC_FAST_CASE(1) SC_FAST_CASE(2) SC_FAST_CASE(3) SC_FAST_CASE(4)
-          SC_FAST_CASE(5) SC_FAST_CASE(6) SC_FAST_CASE(7) SC_FAST_CASE(8)
-          SC_FAST_CASE(9) SC_FAST_CASE(10) SC_FAST_CASE(11) SC_FAST_CASE(12)
-          SC_FAST_CASE(13) SC_FAST_CASE(14) SC_FAST_CASE(15)
-#undef SC_FAST_CASE
-          default:  // kProgNoRecord
-            fast_stage<R, NR, 0>(cur, rbase, tab, q, last, wbase, sidx, dst, gt_last, p);
-            break;
-        }
-        continue;
-      }
-      if constexpr (!kFast) {
-        // the general record loop: one jump per record into code specialised on its
-        // register bits
-        A v[NV];
-#pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
-        RegOff<NR> off;
-#pragma unroll
-        for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
+      for (int k = 0; k < NR; ++k) off.rb[k] = 1u << stg.R[k];
+      // a leading X of the stage's only rotation record is folded into tab.rd
+      const uint32_t folded_x = (uint32_t)tab.xm;
 
 #pragma unroll 1
-        for (int gi = stg.g0;; ++gi) {
-          if constexpr (kBatch) {
-            // the next record to apply: the records a trajectory skips (mostly the
-            // identity choice of a Pauli slot) go by in a scan of their own, off the
-            // loop edge that carries the amplitude registers
+      for (int gi = stg.g0;; ++gi) {
+        if constexpr (kBatch) {
+          // the next record to apply: the records a trajectory skips (mostly the
+          // identity choice of a Pauli slot) go by in a scan of their own, off the
+          // loop edge that carries the amplitude registers
 #pragma unroll 1
-            for (; gi < stg.g1; ++gi) {
-              const SwGate& q = p.gates[gi];
-              if (((uint64_t)base & q.gmask) != q.gmask) continue;
-              if ((q.kind == SK_PAULI || q.kind == SK_PAULIF) && codes[q.b] == 0) continue;
-              break;
-            }
-            if (gi >= stg.g1) break;
-          } else {
-            if (gi >= stg.g1) break;
-            if (((uint64_t)base & p.gates[gi].gmask) != p.gates[gi].gmask) continue;
+          for (; gi < stg.g1; ++gi) {
+            const SwGate& q = p.gates[gi];
+            if (((uint64_t)base & q.gmask) != q.gmask) continue;
+            if ((q.kind == SK_PAULI || q.kind == SK_PAULIF) && codes[q.b] == 0) continue;
+            break;
           }
-          const SwGate& g = p.gates[gi];
-          const R* m = p.pool + g.moff;
-          const uint32_t lmask = g.lmask;
-          switch (g.code) {
+          if (gi >= stg.g1) break;
+        } else {
+          if (gi >= stg.g1) break;
+          if (((uint64_t)base & p.gates[gi].gmask) != p.gates[gi].gmask) continue;
+        }
+        const SwGate& g = p.gates[gi];
+        const R* m = p.pool + g.moff;
+        const uint32_t lmask = g.lmask;
+        switch (g.code) {
 #define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask)
 #define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask)
 #define SC_DO_D1R(A) d1r<R, NR, A>(v, m)
@@ -829,28 +768,28 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
   xfold<NR, A>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
 #define SC_DO_CXF(A, B) \
   cxfold<NR, A, B>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
-            SC_CASES_1(SK_X0, SC_DO_X0)
-            SC_CASES_2(SK_CX0, SC_DO_CX0)
-            SC_CASES_1(SK_XF, SC_DO_XF)
-            SC_CASES_2(SK_CXF, SC_DO_CXF)
+          SC_CASES_1(SK_X0, SC_DO_X0)
+          SC_CASES_2(SK_CX0, SC_DO_CX0)
+          SC_CASES_1(SK_XF, SC_DO_XF)
+          SC_CASES_2(SK_CXF, SC_DO_CXF)
 #undef SC_DO_XF
 #undef SC_DO_CXF
-            SC_CASES_1(SK_PAULI, SC_DO_PAULI)
-            case SK_PAULIF << 4:
-              if constexpr (kBatch) {
-                pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
-              }
-              break;
+          SC_CASES_1(SK_PAULI, SC_DO_PAULI)
+          case SK_PAULIF << 4:
+            if constexpr (kBatch) {
+              pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
+            }
+            break;
 #undef SC_DO_X0
 #undef SC_DO_CX0
 #undef SC_DO_PAULI
-            SC_CASES_1(SK_G1, SC_DO_G1)
-            SC_CASES_1(SK_X, SC_DO_X)
-            SC_CASES_1(SK_D1R, SC_DO_D1R)
-            SC_CASES_2(SK_G2, SC_DO_G2)
-            SC_CASES_2(SK_CX, SC_DO_CX)
-            SC_CASES_2(SK_DPR, SC_DO_DPR)
-            SC_CASES_2(SK_SWAP, SC_DO_SWAP)
+          SC_CASES_1(SK_G1, SC_DO_G1)
+          SC_CASES_1(SK_X, SC_DO_X)
+          SC_CASES_1(SK_D1R, SC_DO_D1R)
+          SC_CASES_2(SK_G2, SC_DO_G2)
+          SC_CASES_2(SK_CX, SC_DO_CX)
+          SC_CASES_2(SK_DPR, SC_DO_DPR)
+          SC_CASES_2(SK_SWAP, SC_DO_SWAP)
 #undef SC_DO_G1
 #undef SC_DO_X
 #undef SC_DO_D1R
@@ -858,47 +797,54 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
 #undef SC_DO_CX
 #undef SC_DO_DPR
 #undef SC_DO_SWAP
-            // commuting 2x2 gates on several register bits, matrices in bit order;
-            // one case per bit set, so the gates run as straight-line code
+          // commuting 2x2 gates on several register bits, matrices in bit order;
+          // one case per bit set, so the gates run as straight-line code
 #define SC_G1ALL_CASE(M)                        \
   case (SK_G1ALL << 4) | (M):                   \
     if constexpr (((M) >> NR) == 0) {           \
       g1all<R, NR, (M)>(v, m, l0, off);         \
     }                                           \
     break;
-            SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
-            SC_G1ALL_CASE(5) SC_G1ALL_CASE(6) SC_G1ALL_CASE(7) SC_G1ALL_CASE(8)
-            SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
-            SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
+          SC_G1ALL_CASE(1) SC_G1ALL_CASE(2) SC_G1ALL_CASE(3) SC_G1ALL_CASE(4)
+          SC_G1ALL_CASE(5) SC_G1ALL_CASE(6) SC_G1ALL_CASE(7) SC_G1ALL_CASE(8)
+          SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
+          SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
 #undef SC_G1ALL_CASE
-#define SC_G1ALLQ_CASE(M)                       \
-  case (SK_G1ALLQ << 4) | (M):                  \
-    if constexpr (((M) >> NR) == 0) {           \
-      if (g.b) prex<R, NR>(v, (uint32_t)g.b);   \
-      g1allq<R, NR, (M)>(v, m);                 \
-    }                                           \
+#define SC_G1ALLQ_CASE(M)                                   \
+  case (SK_G1ALLQ << 4) | (M):                              \
+    if constexpr (((M) >> NR) == 0) {                       \
+      if (g.b && !folded_x) prex<R, NR>(v, (uint32_t)g.b);  \
+      g1allq<R, NR, (M)>(v, m);                             \
+    }                                                       \
     break;
-            SC_G1ALLQ_CASE(1) SC_G1ALLQ_CASE(2) SC_G1ALLQ_CASE(3) SC_G1ALLQ_CASE(4)
-            SC_G1ALLQ_CASE(5) SC_G1ALLQ_CASE(6) SC_G1ALLQ_CASE(7) SC_G1ALLQ_CASE(8)
-            SC_G1ALLQ_CASE(9) SC_G1ALLQ_CASE(10) SC_G1ALLQ_CASE(11) SC_G1ALLQ_CASE(12)
-            SC_G1ALLQ_CASE(13) SC_G1ALLQ_CASE(14) SC_G1ALLQ_CASE(15)
+          SC_G1ALLQ_CASE(1) SC_G1ALLQ_CASE(2) SC_G1ALLQ_CASE(3) SC_G1ALLQ_CASE(4)
+          SC_G1ALLQ_CASE(5) SC_G1ALLQ_CASE(6) SC_G1ALLQ_CASE(7) SC_G1ALLQ_CASE(8)
+          SC_G1ALLQ_CASE(9) SC_G1ALLQ_CASE(10) SC_G1ALLQ_CASE(11) SC_G1ALLQ_CASE(12)
+          SC_G1ALLQ_CASE(13) SC_G1ALLQ_CASE(14) SC_G1ALLQ_CASE(15)
 #undef SC_G1ALLQ_CASE
-            case SK_D1 << 4:
-              diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
-              break;
-            case SK_DP << 4:
-              diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
-              break;
-            case SK_D2 << 4:
-              diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
-              break;
-            default: break;
-          }
+          case SK_DTAB << 4:
+            dtab<R, NR>(v, m);
+            break;
+          case SK_D1 << 4:
+            diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
+            break;
+          case SK_DP << 4:
+            diagp_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+            break;
+          case SK_D2 << 4:
+            diag2_any<R, NR>(v, m, g.a, g.b, l0, off, base);
+            break;
+          default: break;
         }
-        if (!last) __syncthreads();  // every read of `cur` in this stage is done
-        stage_exit<R, NR>(v, last, cur, wbase, tab, sidx, dst, gt_last, p);
       }
     }
+    A* __restrict__ dst = item_state(t) + base;
+    if (p.has_scale) {
+#pragma unroll
+      for (int j = 0; j < NV; ++j) v[j] = cmul(p.scale_re, p.scale_im, v[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < NV; ++j) dst[gt_last | p.glast[j]] = v[j];
   }
   if constexpr (kTma) {
     // a thread that stopped waiting may leave tile copies in flight: thread 0 waits
@@ -968,6 +914,10 @@ __device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 <
     SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
     SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
 #undef SC_G1ALL_CASE
+    case SK_DTAB << 4:
+      dtab<R, NR>(v, m);
+      dtab<R, NR>(w, m);
+      break;
     case SK_D1 << 4:
       diag1_any<R, NR>(v, m, g.a, l0, off, lmask, base);
       diag1_any<R, NR>(w, m, g.a, l0, off, lmask, base);
@@ -1123,7 +1073,7 @@ __global__ void k_probe_reduce(const double* __restrict__ partial, int ctas, int
 
 struct LaunchCache {
   std::mutex mu;
-  bool attr_set[2][SW_MAX_NR + 1][2][2][2] = {};
+  bool attr_set[2][SW_MAX_NR + 1][2][2] = {};
 };
 LaunchCache g_cache;
 
@@ -1288,19 +1238,19 @@ bool check_tile_tensor(SweepParams<R>& p, int64_t* stats) {
   return true;
 }
 
-template <typename R, int NR, bool kTma, bool kBatch, bool kFast>
+template <typename R, int NR, bool kTma, bool kBatch>
 cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_count,
                       cudaStream_t s) {
   using A = typename Amp<R>::type;
-  auto kern = k_sweep<R, NR, kTma, kBatch, kFast>;
+  auto kern = k_sweep<R, NR, kTma, kBatch>;
   const int di = std::is_same<R, float>::value ? 1 : 0;
   {
     std::lock_guard<std::mutex> lk(g_cache.mu);
-    if (!g_cache.attr_set[di][NR][kTma][kBatch][kFast]) {
+    if (!g_cache.attr_set[di][NR][kTma][kBatch]) {
       cudaError_t e =
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
       if (e != cudaSuccess) return e;
-      g_cache.attr_set[di][NR][kTma][kBatch][kFast] = true;
+      g_cache.attr_set[di][NR][kTma][kBatch] = true;
     }
   }
   const int threads = 1 << (p.T - NR);
@@ -1316,21 +1266,14 @@ cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_cou
   return cudaGetLastError();
 }
 
-template <typename R, int NR, bool kTma>
-cudaError_t launch_copy(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
-  bool fast = true;  // every stage a straight-line rotation stage
-  for (int k = 0; k < p.n_stages; ++k) fast = fast && p.tabs[k].prog != kProgGeneric;
-  if (p.batch > 1 || p.n_local_slots > 0)
-    return fast ? launch_nr<R, NR, kTma, true, true>(state, p, err, sm_count, s)
-                : launch_nr<R, NR, kTma, true, false>(state, p, err, sm_count, s);
-  return fast ? launch_nr<R, NR, kTma, false, true>(state, p, err, sm_count, s)
-              : launch_nr<R, NR, kTma, false, false>(state, p, err, sm_count, s);
-}
-
 template <typename R, int NR>
 cudaError_t launch_pick(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
-  if (make_tile_tensor<R>(state, p)) return launch_copy<R, NR, true>(state, p, err, sm_count, s);
-  return launch_copy<R, NR, false>(state, p, err, sm_count, s);
+  const bool batch = p.batch > 1 || p.n_local_slots > 0;
+  if (make_tile_tensor<R>(state, p))
+    return batch ? launch_nr<R, NR, true, true>(state, p, err, sm_count, s)
+                 : launch_nr<R, NR, true, false>(state, p, err, sm_count, s);
+  return batch ? launch_nr<R, NR, false, true>(state, p, err, sm_count, s)
+               : launch_nr<R, NR, false, false>(state, p, err, sm_count, s);
 }
 
 template <typename R>
@@ -1528,13 +1471,14 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
     }
     if (s == 0)
       for (int j = 0; j < 16; ++j) p->off0[j] = off[j];
-    // the stage's code: one rotation record (plus slot folds) runs straight through
+    // a stage whose only register record is one rotation record (other records being
+    // slot folds, which act at the exit) reads its registers with the record's
+    // leading X already applied
     int n_rot = 0, n_other = 0, rot_g = -1;
     for (int g = plan.stages[sw.s0 + s].g0; g < plan.stages[sw.s0 + s].g1; ++g) {
       const SwGate& q = plan.gates[g];
       if (q.kind == SK_XF || q.kind == SK_CXF) continue;
-      if (q.kind == SK_G1ALLQ && q.lmask == 0 && q.gmask == 0 && (q.a & 15) != 0 &&
-          ((q.a & 15) >> sw.nr) == 0) {
+      if (q.kind == SK_G1ALLQ && q.lmask == 0 && q.gmask == 0) {
         ++n_rot;
         rot_g = g;
       } else {
@@ -1542,23 +1486,8 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
       }
     }
     SwStageTab& tb = p->tabs[s];
-    tb.prog = kProgGeneric;
-    tb.qoff = 0;
-    tb.xm = 0;
+    tb.xm = (n_other == 0 && n_rot == 1) ? (plan.gates[rot_g].b & (nv - 1)) : 0;
     tb.pad = 0;
-    static const bool straight = [] {
-      const char* v = getenv("STATECRAFT_B200_FAST_STAGES");
-      return !(v && atoi(v) == 0);
-    }();
-    if (!straight) {
-      // every stage through the record loop
-    } else if (n_other == 0 && n_rot == 1) {
-      tb.prog = plan.gates[rot_g].a & 15;
-      tb.qoff = plan.gates[rot_g].moff - sw.pool0;
-      tb.xm = plan.gates[rot_g].b & (nv - 1);
-    } else if (n_other == 0 && n_rot == 0) {
-      tb.prog = kProgNoRecord;
-    }
     for (int j = 0; j < 16; ++j) {
       const int jx = j < nv ? j ^ tb.xm : j;
       tb.rd[j] = s == 0 ? off[jx] : (uint16_t)apply_swizzle(off[jx], zin[s], K);
@@ -1762,7 +1691,7 @@ bool adjoint_plan_supported(const Plan& plan) {
     for (int g = plan.stages[sw.s0].g0; g < plan.stages[sw.s1 - 1].g1; ++g) {
       switch (plan.gates[g].kind) {
         case SK_G1: case SK_X: case SK_SWAP: case SK_D1: case SK_D2: case SK_DP:
-        case SK_CX: case SK_DPR: case SK_G1ALL: case SK_D1R: case SK_X0: case SK_CX0:
+        case SK_CX: case SK_DPR: case SK_G1ALL: case SK_D1R: case SK_X0: case SK_CX0: case SK_DTAB:
         case SK_PROBE:
           break;
         default: return false;

@@ -273,6 +273,7 @@ uint32_t record_bits(const SwGate& g, const int* reg_of_pos) {
       f |= (1u << g.a) | (1u << g.b);
       break;
     case SK_G1ALL: case SK_G1ALLQ: f |= (uint32_t)g.a & 15u; break;
+    case SK_DTAB: f |= 15u; break;
     case SK_D1: reg(g.a); break;
     case SK_DP: case SK_D2: reg(g.a); reg(g.b); break;
     default: return 0xFFFFFFFFu;
@@ -495,6 +496,43 @@ void optimize_stage(Plan& plan, int32_t g0, SwStage& st, const int* reg_of_pos,
   }
   for (int k = (int)G.size() - 1; k >= g0; --k)
     if (fold[k - g0]) G.erase(G.begin() + k);
+}
+
+// Runs of two or more adjacent register-bit diagonals (D1R / DPR without tile or
+// global controls) become one SK_DTAB record: their product as a table over the
+// stage's 2^nr register indices.  They commute, so the order inside a run is free.
+// pool_limit: the end of the sweep's pool budget (a table that would pass it is not
+// made).
+void merge_register_diagonals(Plan& plan, int32_t g0, int nr, size_t pool_limit) {
+  std::vector<SwGate>& G = plan.gates;
+  for (int i = g0; i < (int)G.size(); ++i) {
+    if (!register_diagonal(G[i])) continue;
+    int j = i;
+    while (j + 1 < (int)G.size() && register_diagonal(G[j + 1])) ++j;
+    if (j == i) continue;
+    if (plan.pool.size() + (2u << nr) > pool_limit) return;
+    SwGate t;
+    std::memset(&t, 0, sizeof t);
+    t.kind = SK_DTAB;
+    t.code = sw_code(SK_DTAB, 0, 0);
+    t.moff = (int32_t)plan.pool.size();
+    std::vector<double> tab(2 * ((size_t)1 << nr));
+    for (int x = 0; x < (1 << nr); ++x) {
+      double pr = 1.0, pi = 0.0;
+      for (int k = i; k <= j; ++k) {
+        double dr, di;
+        diagonal_at(G[k], plan.pool, x, &dr, &di);
+        const double nr_ = pr * dr - pi * di, ni = pr * di + pi * dr;
+        pr = nr_;
+        pi = ni;
+      }
+      tab[2 * x] = pr;
+      tab[2 * x + 1] = pi;
+    }
+    plan.pool.insert(plan.pool.end(), tab.begin(), tab.end());
+    G.erase(G.begin() + i + 1, G.begin() + j + 1);
+    G[i] = t;
+  }
 }
 
 }  // namespace
@@ -1106,6 +1144,7 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       if (pp.peephole)
         optimize_stage(plan, st.g0, st, reg_of_pos, folded_bits, is_last, &sw.scale_re,
                        &sw.scale_im);
+      merge_register_diagonals(plan, st.g0, NR, (size_t)sw.pool0 + (size_t)pp.max_pool);
       plan.gate_ops.insert(plan.gate_ops.end(), folded_ops.begin(), folded_ops.end());
       st.g1 = (int32_t)plan.gates.size();
       plan.stages.push_back(st);

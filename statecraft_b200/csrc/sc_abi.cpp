@@ -38,7 +38,8 @@ int fail_cuda(cudaError_t e, const char* where) {
 const char* kernel_class_name(int cls) {
   static const char* names[KC_COUNT] = {"sweep",  "gate_dense", "gate_perm", "gate_diag",
                                         "init",   "probabilities", "sample",  "noise",
-                                        "expect", "adjoint",    "batch",   "permute"};
+                                        "expect", "adjoint",    "batch",   "permute",
+                                        "block"};
   return (cls >= 0 && cls < KC_COUNT) ? names[cls] : "unknown";
 }
 
@@ -276,6 +277,51 @@ int Ctx::apply_gates(const std::vector<PGate>& gates) {
     }
     return SC_OK;
   }
+  if (dense_block_cost > 0.0 && cfg.dtype == SC_C128) {
+    // runs of gates on at most 5 qubits heavy enough for a dense block go to the
+    // tensor-core kernel; the rest is planned into sweeps run by run
+    std::vector<DenseBlock> blocks;
+    std::vector<GateRun> runs = cut_dense_blocks(gates, n, dense_block_cost, &blocks);
+    if (!blocks.empty()) {
+      size_t elems = 0;
+      for (const DenseBlock& b : blocks) elems += b.u.size();
+      int rc = reserve(buf_block, sizeof(double) * elems, "dense block matrices");
+      if (rc != SC_OK) return rc;
+      std::vector<double> host;
+      host.reserve(elems);
+      std::vector<size_t> offs;
+      for (const DenseBlock& b : blocks) {
+        offs.push_back(host.size());
+        host.insert(host.end(), b.u.begin(), b.u.end());
+      }
+      cudaError_t e = cudaMemcpyAsync(buf_block.p, host.data(), sizeof(double) * elems,
+                                      cudaMemcpyHostToDevice, stream);
+      if (e != cudaSuccess) return fail_cuda(e, "dense block upload");
+      for (const GateRun& r : runs) {
+        if ((rc = apply_sweeps(r.gates)) != SC_OK) return rc;
+        if (r.block < 0) continue;
+        const DenseBlock& b = blocks[(size_t)r.block];
+        mark_begin(KC_BLOCK, 2.0 * dim * amp_bytes);
+        e = launch_block(state.p, n, b.args, static_cast<const double*>(buf_block.p) + offs[(size_t)r.block],
+                         sm_count, stream);
+        mark_end();
+        if (e != cudaSuccess) return fail_cuda(e, "dense block kernel");
+        ++plan_sweeps_count;
+        ++plan_blocks;
+        plan_gates += b.n_gates;
+      }
+      // the host copy must outlive the upload
+      if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) return fail_cuda(e, "dense blocks");
+      return SC_OK;
+    }
+  }
+  return apply_sweeps(gates);
+}
+
+int Ctx::apply_sweeps(const std::vector<PGate>& gates) {
+  if (gates.empty()) return SC_OK;
+  const double amp_bytes = (cfg.dtype == SC_C64) ? 8.0 : 16.0;
+  const double dim = std::ldexp(1.0, n);
   Plan plan = plan_sweeps(gates, n, plan_params());
   if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
   for (size_t k = 0; k < plan.sweeps.size(); ++k) {
@@ -322,7 +368,7 @@ int Ctx::run(int nq, const sc_op* ops, int64_t n_ops, const double* init, uint64
   if ((rc = ensure_state(nq)) != SC_OK) return rc;
   if ((rc = reserve(buf_err, 16, "error flag")) != SC_OK) return rc;
   cudaMemsetAsync(buf_err.p, 0, 16, stream);
-  plan_sweeps_count = plan_gates = plan_stages = 0;
+  plan_sweeps_count = plan_gates = plan_stages = plan_blocks = 0;
 
   // state preparation (populateFromState / resetBasisState / resetZeroState)
   const double dim = std::ldexp(1.0, nq);
@@ -473,6 +519,8 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
   if (const char* v = getenv("STATECRAFT_B200_ROTATION")) c->rotation = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_PEEPHOLE")) c->peephole = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_ADJOINT_FUSED")) c->adjoint_fused = atoi(v) != 0;
+  // minimum sweep-path cost of a dense block (FMA per amplitude); 0 turns blocks off
+  if (const char* v = getenv("STATECRAFT_B200_DENSE_BLOCKS")) c->dense_block_cost = atof(v);
   *out_ctx = c;
   return SC_OK;
 }

@@ -41,6 +41,9 @@ struct Ctx {
   bool rotation = true;  // rotation form for 1-qubit unitaries in sweeps
   bool peephole = true;  // per-stage record peephole in the planner
   bool adjoint_fused = true;  // adjoint reverse pass as dual-state sweeps when it fits
+  // runs of gates on <= 5 qubits whose sweep-path cost (FMA per amplitude) reaches this
+  // become dense tensor-core blocks (complex128; 0 = never)
+  double dense_block_cost = 160.0;
 
   // state
   int n = 0;
@@ -62,6 +65,7 @@ struct Ctx {
   DevBuf buf_expect;                            // Pauli partial sums
   DevBuf buf_adj_phi, buf_adj_lambda;           // adjoint work states
   DevBuf buf_traj_states, buf_traj_aux;         // trajectory batches: states | codes, sampling
+  DevBuf buf_block;                             // dense block matrices of a run
 
   // adjoint bookkeeping
   std::vector<sc_op> adj_ops;
@@ -74,7 +78,7 @@ struct Ctx {
   std::vector<void*> qaoa_batches;
 
   // plan statistics of the last run
-  int64_t plan_sweeps_count = 0, plan_gates = 0, plan_stages = 0;
+  int64_t plan_sweeps_count = 0, plan_gates = 0, plan_stages = 0, plan_blocks = 0;
 
   // timing
   struct Timed {
@@ -94,7 +98,8 @@ struct Ctx {
   void release_all() {
     for (DevBuf* b : {&state, &buf_err, &buf_convert, &buf_noise_state,
                       &buf_noise_partial, &buf_sample, &buf_probs, &buf_marg, &buf_expect,
-                      &buf_adj_phi, &buf_adj_lambda, &buf_traj_states, &buf_traj_aux})
+                      &buf_adj_phi, &buf_adj_lambda, &buf_traj_states, &buf_traj_aux,
+                      &buf_block})
       release(*b);
   }
   void mark_begin(int cls, double bytes, int kernels = 1);
@@ -105,6 +110,7 @@ struct Ctx {
   PlanParams plan_params() const;
   int ensure_state(int nq);
   int apply_gates(const std::vector<PGate>& gates);
+  int apply_sweeps(const std::vector<PGate>& gates);
   int run(int nq, const sc_op* ops, int64_t n_ops, const double* init, uint64_t basis,
           bool has_basis, const double* params, int64_t n_params);
   int sample(const int32_t* qubits, int32_t m, int64_t shots, uint64_t seed,

@@ -264,6 +264,9 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
                 if (const int sub = subset(j)) v[j] = cm(phi[2 * (sub - 1)], phi[2 * (sub - 1) + 1], v[j]);
               break;
             }
+            case SK_DTAB:
+              for (int j = 0; j < NV; ++j) v[j] = cm(m[2 * j], m[2 * j + 1], v[j]);
+              break;
             case SK_D1R:
               for (int j = 0; j < NV; ++j) {
                 const int k = (j >> g.a) & 1;

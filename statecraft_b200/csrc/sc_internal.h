@@ -85,9 +85,12 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        last: applied to the stage's exit slots instead of the registers.
 // SK_PROBE: gradient probe on register bit a, generator Pauli in the code's low two
 //        bits (1 = X, 2 = Y, 3 = Z), b = gradient slot (the adjoint reverse sweep).
+// SK_DTAB: a diagonal over the stage's register bits as a table of 2^NR complex
+//        factors (register j is multiplied by entry j): adjacent register-bit
+//        diagonals of a stage merged into one record.
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF, SK_DTAB
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
@@ -214,6 +217,7 @@ enum KernelClass : int32_t {
   KC_ADJOINT,
   KC_BATCH,
   KC_PERMUTE,
+  KC_BLOCK,
   KC_COUNT
 };
 const char* kernel_class_name(int cls);
@@ -253,6 +257,30 @@ bool check_tile_tensors(const Plan& plan, int dtype, int64_t batch, int64_t* sta
 cudaError_t launch_adjoint_sweep(int dtype, void* psi, void* lam, const Plan& plan, size_t k,
                                  double* partial, int max_ctas, double* grad, int sm_count,
                                  cudaStream_t s);
+// Dense blocks (k_block.cu, sc_blocks.cpp): a run of gates touching k (3..5) qubits
+// composed into one 2^k x 2^k complex unitary, applied with FP64 tensor-core tiles.
+struct BlockArgs {
+  int32_t k;
+  int32_t q[5];  // the block's qubits, ascending; local bit b <-> qubit q[b]
+};
+struct DenseBlock {
+  BlockArgs args;
+  int32_t n_gates;
+  std::vector<double> u;  // 2^k x 2^k row-major, (re, im) pairs
+};
+// One item of a gate stream cut into sweep-planned runs and dense blocks.
+struct GateRun {
+  std::vector<PGate> gates;  // planned into sweeps (may be empty)
+  int block = -1;            // index into the block list, applied after `gates`
+};
+// Cuts `gates` into runs and blocks: consecutive gates whose touched qubits fit in
+// 5 form a block when their summed gate_cost is at least min_cost (FMA per
+// amplitude) and they touch at least 3 qubits; everything else stays in runs.
+std::vector<GateRun> cut_dense_blocks(const std::vector<PGate>& gates, int n, double min_cost,
+                                      std::vector<DenseBlock>* blocks);
+// u: device copy of the block's matrix (2 * 4^k doubles); complex128 states only
+cudaError_t launch_block(void* state, int n, const BlockArgs& a, const double* u, int sm_count,
+                         cudaStream_t s);
 // in-place qubit-bit permutation of an n-qubit state
 cudaError_t launch_permute(int dtype, void* state, int n, const SwPerm& perm, int sm_count,
                            cudaStream_t s);

@@ -16,30 +16,21 @@ constexpr int kSweepMaxPool = 2048;  // matrix reals
 // of register j (the OR of 1 << R[k] over the set bits k of j); rd[j] is the slot
 // register j is read from, relative to the stage's read base (the thread's l0 in
 // the linear layout for stage 0, its swizzled l0 otherwise): the slot of tile
-// offset off[j ^ xm], xm being an X on register bits that the stage's rotation
-// record starts with and that is folded into the read (0 elsewhere).  wsoff[j] is
-// the slot register j is written to when the stage ends (register perm[j] in the
-// next stage's layout) and xoff[a] the offset of register bit a in that layout
-// (slot folds).  Each exchange between two stages has its own XOR swizzle,
-// slot(i) = i ^ sum_k parity(i & rows[k]) << k over the low K slot bits (K = log2
-// of the amplitudes per 128-byte row); rows[] only read bits >= K, so every
-// swizzle is a bijection and XOR-linear over disjoint bits.  rows[] here is the
-// swizzle of the layout this stage reads; bit 15 of rows[0] marks one that differs
-// from the fixed default (rows[k] = 1 << (K + k)).
-// prog selects the stage's code: 0 = the general record loop; 1..15 = a stage whose
-// only register record is one rotation-form record on register-bit mask prog (pool
-// offset qoff), any other records being slot folds; 16 = a stage with slot folds
-// only.  Such a stage runs as straight-line code from its shared-memory read to its
-// exit store.
-constexpr int kProgGeneric = 0;
-constexpr int kProgNoRecord = 16;
+// offset off[j ^ xm], xm being the leading X of the stage's rotation record when
+// that record is the stage's only register record (folded into the read; the
+// record then skips it), else 0.  wsoff[j] is the slot register j is written to
+// when the stage ends (register perm[j] in the next stage's layout) and xoff[a] the
+// offset of register bit a in that layout (slot folds).  Each exchange between two
+// stages has its own XOR swizzle, slot(i) = i ^ sum_k parity(i & rows[k]) << k over
+// the low K slot bits (K = log2 of the amplitudes per 128-byte row); rows[] only
+// read bits >= K, so every swizzle is a bijection and XOR-linear over disjoint bits.
+// rows[] here is the swizzle of the layout this stage reads; bit 15 of rows[0]
+// marks one that differs from the fixed default (rows[k] = 1 << (K + k)).
 struct SwStageTab {
   uint16_t rd[16];
   uint16_t wsoff[16];
   uint16_t xoff[4];
   uint16_t rows[4];
-  int32_t prog;
-  int32_t qoff;
   int32_t xm;
   int32_t pad;
 };

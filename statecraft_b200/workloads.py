@@ -100,6 +100,38 @@ def amp_updates(circuit: Q.QuantumCircuit) -> float:
     return total
 
 
+def dense_window_circuit(n: int, depth: int, seed: int) -> Q.QuantumCircuit:
+    """Hadamards, then `depth` rounds of 12 gates inside a random 5-qubit window:
+    dense random two-qubit unitaries, CNOTs, random single-qubit gates and
+    controlled phases; every third round ends with a multi-controlled Z on all
+    qubits.  Runs of gates on at most 5 qubits with much dense work: the shape the
+    tensor-core blocks are for."""
+    rng = np.random.default_rng(seed)
+    c = Q.QuantumCircuit(n)
+    for q in range(n):
+        c = c.append(Q.Hadamard(), q)
+    for d in range(depth):
+        lo = int(rng.integers(0, n - 4))
+        for _ in range(12):
+            a, b = (int(x) + lo for x in rng.choice(5, 2, replace=False))
+            kind = int(rng.integers(0, 4))
+            if kind == 0:
+                z = (rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))) / np.sqrt(2)
+                qm, r = np.linalg.qr(z)
+                m = qm * (np.diag(r) / np.abs(np.diag(r)))
+                c = c.appendTwoQubitUnitary(list(m.reshape(-1)), a, b)
+            elif kind == 1:
+                c = c.append(Q.CnotGate.of(), a, b)
+            elif kind == 2:
+                th, ph, la = rng.uniform(0, TWO_PI, 3)
+                c = c.append(Q.u3(float(th), float(ph), float(la)), a)
+            else:
+                c = c.appendControlledPhase(float(rng.uniform(0, TWO_PI)), a, b)
+        if d % 3 == 2:
+            c = c.appendMultiControl(Q.PauliZ(), n - 1, *range(n - 1))
+    return c
+
+
 # ---------------------------------------------------------------------------
 # batched QAOA
 # ---------------------------------------------------------------------------
