@@ -17,13 +17,16 @@
 // chunks of kChunk probabilities approximately (FP64); pass B turns them into
 // approximate running sums, which tell which chunks lie inside one binade (with a
 // margin far above the summation error); pass C computes each such chunk's effect in
-// integers; pass D walks the chunks in order from S = 0 -- one integer step per
-// clean chunk, element by element (exact FP64 adds) for the few chunks that cross a
-// binade, start near zero or end the array -- and records the exact running sum
-// before each chunk, the exact total and the rescaling decision; when the reference
-// rescales, passes A-D run again on the rescaled probabilities.  Pass E gives each
-// shot a warp that binary-searches the exact chunk starts and replays its chunk: lane
-// effects, a warp scan, then exact FP64 adds within each lane.
+// integers (a chunk of zeros is the identity anywhere); pass D goes through the chunks
+// in order from S = 0 -- runs of chunks in the running sum's binade as one scan of
+// their effects, and the few chunks that cross a binade, start near zero or end the
+// array by a warp that splits them the same way into 32 segments and adds one by one
+// only inside the segments that cross -- and records the exact running sum before each
+// chunk, the exact total and the rescaling decision; when the reference rescales,
+// passes A-D run again on the rescaled probabilities.  Pass E gives each shot a warp
+// that binary-searches the exact chunk starts and replays its chunk: the exact start
+// of each lane's segment (lane effects and a warp scan), then exact FP64 adds within
+// each lane.
 #include <cfloat>
 
 #include "sc_device.cuh"
@@ -125,7 +128,10 @@ __global__ void __launch_bounds__(1024) k_prefix_approx(const double* sums, uint
 }
 
 // ---- integer form of the running sum inside one binade --------------------------
-constexpr int32_t kTfUsable = 4, kTfApplied = 8;  // ChunkTf::flags bits 2 and 3
+// ChunkTf::flags bits 2-4: an effect that holds in binade e; the effect applied (the
+// chunk's start is the exact running sum and the chunk stays in binade e, or the chunk
+// is all zeros); a chunk of zeros
+constexpr int32_t kTfUsable = 4, kTfApplied = 8, kTfZero = 16;
 
 // effect of a run of additions on A (the running sum in ulps of one binade)
 struct Tf {
@@ -226,6 +232,97 @@ __device__ __forceinline__ bool tf_apply(const Tf& t, int e, double* s) {
   return true;
 }
 
+// The exact FP64 running sum over n <= 32 * PER values in order, from an exact start S,
+// by one warp (every lane calls it; S uniform).  Lane l owns values [l PER, (l+1) PER)
+// and gets back the exact running sum before its first value; *end gets the exact sum
+// after all n.  Lanes whose segment stays inside one binade (approximate sums with a
+// 2^-18 relative margin, far above their error) contribute integer effects; runs of
+// such lanes in the binade of the running sum are one warp scan, and every other lane
+// adds its values one by one from its exact start (in turn, so the work in sequence is
+// the segments that cross a binade or start near zero).
+template <int PER, typename Get>
+__device__ double warp_exact_starts(const Get& get, uint32_t n, double S, int lane,
+                                    double* end) {
+  constexpr double kMargin = 0x1p-18;
+  const uint32_t lb = (uint32_t)lane * PER;
+  double a = 0.0;
+  for (int q = 0; q < PER; ++q) {
+    if (lb + q >= n) break;
+    a += get(lb + q);
+  }
+  double incl = a;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const double ap_start = S + (incl - a), ap_end = S + incl;
+  int e = binade(ap_start * (1.0 - kMargin));
+  bool clean = e > -1000 && binade(ap_start) == e && binade(ap_end * (1.0 + kMargin)) == e;
+  Tf t = tf_identity();
+  if (clean) {
+    bool bad = false;
+    for (int q = 0; q < PER; ++q) {
+      if (lb + q >= n) break;
+      t = tf_compose(t, tf_of(get(lb + q), e, &bad));
+    }
+    clean = !bad;
+  }
+  double mine = S;
+  // a run whose exact application fails (not expected under the margin) sends the
+  // warp round again with every lane adding its own values
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    if (attempt == 1) clean = false;
+    double Sx = S;  // exact running sum before lane L
+    bool fail = false;
+    for (int L = 0; L < 32;) {
+      const int eL = __shfl_sync(0xffffffffu, e, L);
+      const uint32_t ok = __ballot_sync(0xffffffffu, clean && e == eL && lane >= L);
+      // lanes L .. D-1: one run of clean lanes in the binade of the running sum
+      int D = L;
+      if (binade(Sx) == eL) {
+        const uint32_t rest = ~(ok >> L);
+        D = rest ? L + __ffs(rest) - 1 : 32;
+        if (D > 32) D = 32;
+      }
+      if (D > L) {
+        const bool in = lane >= L && lane < D;
+        const Tf ti = tf_warp_scan(in ? t : tf_identity(), lane);
+        Tf te = tf_shfl_up(ti, 1);
+        if (lane == 0) te = tf_identity();
+        if (in) {
+          double s = Sx;
+          if (!tf_apply(te, eL, &s)) fail = true;
+          mine = s;
+        }
+        double se = Sx;
+        const bool ok_end = tf_apply(ti, eL, &se);
+        Sx = __shfl_sync(0xffffffffu, se, D - 1);
+        if (!__shfl_sync(0xffffffffu, ok_end, D - 1)) fail = true;
+        L = D;
+      }
+      if (L < 32) {
+        double s = Sx;
+        if (lane == L) {
+          mine = Sx;
+          for (int q = 0; q < PER; ++q) {
+            if (lb + q >= n) break;
+            s = __dadd_rn(s, get(lb + q));
+          }
+        }
+        Sx = __shfl_sync(0xffffffffu, s, L);
+        ++L;
+      }
+    }
+    if (!__any_sync(0xffffffffu, fail)) {
+      *end = Sx;
+      return mine;
+    }
+  }
+  *end = S;  // not reached: the second attempt adds every value one by one
+  return mine;
+}
+
 // pass C: per chunk, the binade its running sum stays in (from the approximate
 // running sums, with a margin of 2^-18 relative, far above the summation error of at
 // most 2^32 * 2^-53 relative) and its effect there
@@ -259,13 +356,24 @@ __global__ void __launch_bounds__(kThreadsA) k_chunk_tf(Src src, uint64_t len_pe
     }
     __syncthreads();
     const int e = s_e;
+    const uint64_t b0 = cl * kChunk + (uint64_t)threadIdx.x * (kChunk / kThreadsA);
+    const uint64_t off = st * len_per;
     if (e < -1000) {
-      if (threadIdx.x == 0) out[c] = ChunkTf{0, 0, 0, 0};
+      // a chunk of zeros is the identity whatever the running sum (a sum of values
+      // >= 0 is zero only when every value is)
+      bool nz = false;
+      for (int k = 0; k < kChunk / kThreadsA; ++k) {
+        const uint64_t i = b0 + k;
+        if (i >= len_per) break;
+        double pv = src(off + i);
+        if (scaled_pass) pv = __dmul_rn(pv, scale);
+        nz = nz || pv != 0.0;
+      }
+      const bool any_nz = __syncthreads_or(nz);
+      if (threadIdx.x == 0) out[c] = ChunkTf{0, 0, any_nz ? 0 : (2 | kTfZero), -2000};
       __syncthreads();
       continue;
     }
-    const uint64_t b0 = cl * kChunk + (uint64_t)threadIdx.x * (kChunk / kThreadsA);
-    const uint64_t off = st * len_per;
     bool bad = false;
     Tf t = tf_identity();
     for (int k = 0; k < kChunk / kThreadsA; ++k) {
@@ -294,10 +402,12 @@ __global__ void __launch_bounds__(kThreadsA) k_chunk_tf(Src src, uint64_t len_pe
 // pass D (one CTA per state): the exact running sum before each chunk, in chunk
 // order from S = 0; the exact total, the rescaling decision and the status.  On the
 // rescaled pass, only the states the reference rescales.  Chunks go in blocks of
-// 1024: a block whose records all lie in the binade of the running sum is one
-// in-order scan of their effects (each thread then applies its exclusive prefix to
-// the block's start); any other block is walked by thread 0, record by record, and
-// the whole CTA joins in to stage each chunk that is added element by element.
+// 1024 records.  Within a block the CTA alternates two steps: the longest run of
+// records from the current one whose effects hold in the binade of the running sum
+// (chunks of zeros hold in any) is one in-order scan of their effects, each thread
+// applying its exclusive prefix to the exact running sum; the record that ends the run
+// is staged in shared memory by the CTA and added exactly by warp 0 (lane effects where
+// they hold, one by one elsewhere).
 template <typename Src>
 __global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per,
                                                        uint64_t chunks_per, ChunkTf* tfs,
@@ -310,97 +420,93 @@ __global__ void __launch_bounds__(1024) k_exact_starts(Src src, uint64_t len_per
   starts += st * chunks_per;
   const uint64_t off = st * len_per;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nwarps = (int)(blockDim.x >> 5);
   __shared__ ChunkTf blk[1024];
   __shared__ double elems[kChunk];
   __shared__ Tf wsum[32];
-  __shared__ uint32_t s_next;
-  __shared__ int s_all_ok;
-  __shared__ double s_S;  // the running sum at the start of the current block
+  __shared__ uint32_t s_d;
+  __shared__ double s_S;  // the exact running sum before record k
   if (threadIdx.x == 0) s_S = 0.0;
   for (uint64_t c0 = 0; c0 < chunks_per; c0 += 1024) {
     const uint32_t n_blk = (uint32_t)min((uint64_t)1024, chunks_per - c0);
     __syncthreads();
-    if (threadIdx.x == 0) s_all_ok = 1;
     if (threadIdx.x < n_blk) blk[threadIdx.x] = tfs[c0 + threadIdx.x];
-    __syncthreads();
-    // the scan path: every record usable and in the binade of the running sum
-    const double S0 = s_S;
-    const int e0 = binade(S0);
-    Tf t = tf_identity();
-    if (threadIdx.x < n_blk) {
-      const ChunkTf& r = blk[threadIdx.x];
-      if (!(r.flags & kTfUsable) || r.e != e0) s_all_ok = 0;
-      t = Tf{r.d0, r.d1, (uint32_t)(r.flags & 3)};
-    }
-    __syncthreads();
-    if (s_all_ok && e0 > -1000) {
-      const Tf incl = tf_warp_scan(t, lane);
-      if (lane == 31) wsum[warp] = incl;
+    for (uint32_t k = 0; k < n_blk;) {
+      if (threadIdx.x == 0) s_d = n_blk;
       __syncthreads();
+      const double S = s_S;
+      const int e = binade(S);
+      const uint32_t i = threadIdx.x;
+      bool zero = false, in = false;
+      Tf t = tf_identity();
+      if (i >= k && i < n_blk) {
+        const ChunkTf& r = blk[i];
+        zero = (r.flags & kTfZero) != 0;
+        in = zero || ((r.flags & kTfUsable) && r.e == e && e > -1000);
+        if (in && !zero) t = Tf{r.d0, r.d1, (uint32_t)(r.flags & 3)};
+        if (!in) atomicMin(&s_d, i);
+      }
+      // in-order scan of the effects over the block (identity outside [k, n_blk))
+      const Tf incl_w = tf_warp_scan(t, lane);
+      if (lane == 31) wsum[warp] = incl_w;
+      __syncthreads();
+      const uint32_t D = s_d;
       if (warp == 0) {
-        const Tf w = tf_warp_scan(lane < (int)(blockDim.x >> 5) ? wsum[lane] : tf_identity(), lane);
+        const Tf w = tf_warp_scan(lane < nwarps ? wsum[lane] : tf_identity(), lane);
+        __syncwarp();
         wsum[lane] = w;  // inclusive over warps
       }
       __syncthreads();
-      Tf excl = tf_shfl_up(incl, 1);
-      if (lane == 0) excl = tf_identity();
-      if (warp > 0) excl = tf_compose(wsum[warp - 1], excl);
-      // the whole block stays in the binade when its total does (increments are >= 0)
-      double end = S0;
-      const bool fits = tf_apply(wsum[(blockDim.x >> 5) - 1], e0, &end);
-      if (fits) {
-        if (threadIdx.x < n_blk) {
-          double sv = S0;
-          tf_apply(excl, e0, &sv);
-          starts[c0 + threadIdx.x] = sv;
-          tfs[c0 + threadIdx.x].flags = blk[threadIdx.x].flags | kTfApplied;
+      if (D > k) {
+        Tf excl = tf_shfl_up(incl_w, 1);
+        if (lane == 0) excl = tf_identity();
+        if (warp > 0) excl = tf_compose(wsum[warp - 1], excl);
+        const Tf incl = tf_compose(excl, t);
+        // the run ends early where an effect does not keep the exact sum in the binade
+        // (not expected: the records' binades carry a margin)
+        double sv = S, se = S;
+        bool ok_s = true, ok_e = true;
+        if (e > -1000) {
+          ok_s = tf_apply(excl, e, &sv);
+          ok_e = tf_apply(incl, e, &se);
         }
+        if (i >= k && i < D && !ok_e) atomicMin(&s_d, i);
         __syncthreads();
-        if (threadIdx.x == 0) s_S = end;
-        continue;
-      }
-    }
-    double S = S0;  // thread 0's running sum on the walk path
-    for (uint32_t k = 0; k < n_blk;) {
-      if (threadIdx.x == 0) {
-        // apply chunk records while they keep the sum in their binade
-        uint32_t q = k;
-        for (; q < n_blk; ++q) {
-          ChunkTf& r = blk[q];
-          if (!(r.flags & kTfUsable) || binade(S) != r.e) break;
-          const Tf tq{r.d0, r.d1, (uint32_t)(r.flags & 3)};
-          double Sn = S;
-          if (!tf_apply(tq, r.e, &Sn)) break;
-          starts[c0 + q] = S;
-          S = Sn;
-          r.flags |= kTfApplied;
+        const uint32_t D2 = s_d;
+        if (i >= k && i < D2) {
+          starts[c0 + i] = sv;
+          blk[i].flags |= kTfApplied;
+          (void)ok_s;
         }
-        s_next = q;
+        if (D2 > k && i == D2 - 1) s_S = se;
+        __syncthreads();
+        k = D2;
+        if (k >= n_blk) break;
       }
-      __syncthreads();
-      k = s_next;
-      if (k >= n_blk) break;
-      // chunk k: element by element, exact FP64 adds in the reference's order
+      // record k: its chunk staged, then added exactly by warp 0
       const uint64_t b = (c0 + k) * kChunk;
-      for (int q = threadIdx.x; q < kChunk; q += blockDim.x) {
-        const uint64_t i = b + q;
-        double pv = i < len_per ? src(off + i) : 0.0;
+      const uint32_t lim = (uint32_t)min((uint64_t)kChunk, len_per - b);
+      for (uint32_t q = threadIdx.x; q < lim; q += blockDim.x) {
+        double pv = src(off + b + q);
         if (scaled_pass) pv = __dmul_rn(pv, scale);
         elems[q] = pv;
       }
       __syncthreads();
-      if (threadIdx.x == 0) {
-        starts[c0 + k] = S;
-        blk[k].flags &= ~kTfApplied;
-        const uint64_t lim = min((uint64_t)kChunk, len_per - b);
-        for (uint64_t q = 0; q < lim; ++q) S = __dadd_rn(S, elems[q]);
+      if (warp == 0) {
+        const double S0 = s_S;
+        double end = S0;
+        warp_exact_starts<kChunk / 32>([&](uint32_t q) { return elems[q]; }, lim, S0, lane,
+                                       &end);
+        if (lane == 0) {
+          starts[c0 + k] = S0;
+          blk[k].flags &= ~kTfApplied;
+          s_S = end;
+        }
       }
-      __syncthreads();
       ++k;
     }
     __syncthreads();
     if (threadIdx.x < n_blk) tfs[c0 + threadIdx.x].flags = blk[threadIdx.x].flags;
-    if (threadIdx.x == 0) s_S = S;
   }
   __syncthreads();
   if (threadIdx.x == 0 && !scaled_pass) {
@@ -459,12 +565,12 @@ __global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
     }
     const uint64_t b = (uint64_t)j * kChunk;
     const ChunkTf rec = tfs[j];
-    uint64_t found = ~0ULL;
-    if (rec.flags & kTfApplied) {
-      // the chunk's sum stays in binade rec.e: each lane's start from the lanes'
-      // effects, then exact FP64 adds inside the lane
-      constexpr int per = kChunk / 32;
-      const uint64_t lb = b + (uint64_t)lane * per;
+    constexpr int per = kChunk / 32;
+    const uint64_t lb = b + (uint64_t)lane * per;
+    // the exact running sum before this lane's values
+    double run = starts[j];
+    if ((rec.flags & kTfApplied) && !(rec.flags & kTfZero)) {
+      // the chunk's sum stays in binade rec.e: the lanes' effects, scanned
       bool bad = false;
       Tf t = tf_identity();
       for (int q = 0; q < per; ++q) {
@@ -475,34 +581,27 @@ __global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
       const Tf incl = tf_warp_scan(t, lane);
       Tf excl = tf_shfl_up(incl, 1);
       if (lane == 0) excl = tf_identity();
-      double run = starts[j];
       tf_apply(excl, rec.e, &run);
-      for (int q = 0; q < per; ++q) {
-        const uint64_t i = lb + q;
-        if (i >= len) break;
-        run = __dadd_rn(run, prob(i));
-        if (i == len - 1 || run >= u) {  // the last entry is 1.0
-          found = i;
-          break;
-        }
+    } else if (!(rec.flags & kTfApplied)) {
+      // a chunk that crosses a binade, starts near zero or ends the array
+      double end;
+      run = warp_exact_starts<per>([&](uint32_t q) { return prob(b + q); },
+                                   (uint32_t)min((uint64_t)kChunk, len - b), run, lane, &end);
+    }
+    uint64_t found = ~0ULL;
+    for (int q = 0; q < per; ++q) {
+      const uint64_t i = lb + q;
+      if (i >= len) break;
+      run = __dadd_rn(run, prob(i));
+      if (i == len - 1 || run >= u) {  // the last entry is 1.0
+        found = i;
+        break;
       }
+    }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const uint64_t y = __shfl_xor_sync(0xffffffffu, found, o);
-        found = y < found ? y : found;
-      }
-    } else if (lane == 0) {
-      // element by element from the chunk's exact start
-      double run = starts[j];
-      const uint64_t lim = min((uint64_t)kChunk, len - b);
-      for (uint64_t q = 0; q < lim; ++q) {
-        const uint64_t i = b + q;
-        run = __dadd_rn(run, prob(i));
-        if (i == len - 1 || run >= u) {
-          found = i;
-          break;
-        }
-      }
+    for (int o = 16; o > 0; o >>= 1) {
+      const uint64_t y = __shfl_xor_sync(0xffffffffu, found, o);
+      found = y < found ? y : found;
     }
     if (lane == 0) {
       uint64_t r = found;

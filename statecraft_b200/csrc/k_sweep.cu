@@ -615,6 +615,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
     if (tid == 0) {
       mbar_init(&bars[0], 1);
       mbar_init(&bars[1], 1);
+      mbar_init(&bars[2], 1);  // arrived on by nobody: the test hook's wait
       mbar_init_fence();
     }
     __syncthreads();
@@ -670,7 +671,9 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
         issue_load(tn, b ^ 1);
         issued = i + 2;
       }
-      if (!timed_out && !mbar_wait_bounded(&bars[b], (i >> 1) & 1u, kWaitLimitCycles)) {
+      const bool stall = p.stall_first > 0 && i == 0;
+      if (!timed_out && !mbar_wait_bounded(stall ? &bars[2] : &bars[b], stall ? 0u : (i >> 1) & 1u,
+                                           stall ? (long long)p.stall_first : kWaitLimitCycles)) {
         timed_out = true;
         atomicExch(err, 1);
       }
@@ -1269,6 +1272,8 @@ cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_cou
 template <typename R, int NR>
 cudaError_t launch_pick(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
   const bool batch = p.batch > 1 || p.n_local_slots > 0;
+  p.stall_first = 0;
+  if (const char* v = getenv("STATECRAFT_B200_TEST_STALL_CYCLES")) p.stall_first = atoi(v);
   if (make_tile_tensor<R>(state, p))
     return batch ? launch_nr<R, NR, true, true>(state, p, err, sm_count, s)
                  : launch_nr<R, NR, true, false>(state, p, err, sm_count, s);
@@ -1409,6 +1414,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
   const int g_lo = plan.stages[sw.s0].g0, g_hi = plan.stages[sw.s1 - 1].g1;
   if (g_hi - g_lo > kSweepMaxGates) return false;
   p->tm_rank = 0;
+  p->stall_first = 0;
   p->T = sw.T;
   p->L = sw.L;
   p->h = sw.h;

@@ -49,6 +49,9 @@ template <typename R>
 struct SweepParams {
   alignas(64) uint64_t tmap[16];  // CUtensorMap (opaque, 128 bytes) when tm_rank > 0
   int32_t tm_rank;
+  // failure-detection test hook: when > 0, each CTA's first tile wait is on a barrier
+  // nothing arrives on, bounded by this many cycles (the wait runs out)
+  int32_t stall_first;
   int32_t tm_shift[kTileTensorMaxRank];
   uint32_t tm_mask[kTileTensorMaxRank];
   int32_t T, L, h, nr;

@@ -192,6 +192,43 @@ def test_sampling_dyadic_probabilities_with_ties(fused):
     np.testing.assert_array_equal(got, want)
 
 
+def _sparse_probabilities(kind, n, rng):
+    p = np.zeros(1 << n)
+    if kind == "ghz":
+        p[0] = p[-1] = 0.5
+    elif kind == "last":
+        p[-1] = 1.0
+    elif kind == "middle":
+        p[rng.integers(17 * 2048, 18 * 2048, 5)] = rng.random(5)
+    elif kind == "tiny_head":
+        p[:300] = 1e-300
+        p[300:310] = rng.random(10)
+        p[5000:5003] = 2.0 ** -1070  # subnormal steps on a normal sum
+    elif kind == "zero_chunks":
+        keep = rng.random((1 << n) // 2048) < 0.1
+        p = rng.random(1 << n) * np.repeat(keep, 2048)
+    return p / p.sum()
+
+
+@pytest.mark.parametrize("kind", ["ghz", "last", "middle", "tiny_head", "zero_chunks"])
+def test_sampling_sparse_states(kind, fused):
+    # chunks of zeros before, between and after the mass; a running sum that starts
+    # at tiny values; all the mass in the last chunk
+    n = 16
+    rng = np.random.default_rng(31)
+    p = _sparse_probabilities(kind, n, rng)
+    init = np.zeros(2 << n)
+    init[0::2] = np.sqrt(p)
+    ctx = fused.context()
+    ctx.run_ops(n, *serialize_circuit(Q.QuantumCircuit(n)), init)
+    cdf = O.cumulative(O.probabilities(init, n, list(range(n))))
+    nz = np.flatnonzero(np.diff(np.concatenate([[0.0], cdf])))
+    u = np.concatenate([rng.random(3000), cdf[nz], np.nextafter(cdf[nz], 0), [0.0]])
+    got = ctx.sample(list(range(n)), u.size, None, u)
+    want = O.sample(init, n, list(range(n)), u.size, 0, u)
+    np.testing.assert_array_equal(got, want)
+
+
 def test_tie_rule_and_last_entry(fused):
     # state with exact probabilities 1/4, 0, 1/4, 1/2 on 2 qubits
     init = np.array([0.5, 0, 0, 0, 0.5, 0, math.sqrt(0.5), 0])
