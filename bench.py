@@ -56,6 +56,9 @@ def parse_args(argv=None):
                          "noisy-trajectory workloads (one JSON line each, 1 GPU)")
     ap.add_argument("--instances", type=int, default=4096, help="QAOA batch size")
     ap.add_argument("--trajectories", type=int, default=1024, help="trajectory batch size")
+    ap.add_argument("--channel", choices=["depolarizing", "amplitude_damping"],
+                    default="depolarizing", help="trajectories: noise channel")
+    ap.add_argument("--autotune", action="store_true", help="trajectories: time tile shapes")
     ap.add_argument("--no-tune", action="store_true", help="QAOA: fixed kernel shape")
     return ap.parse_args(argv)
 
@@ -357,35 +360,60 @@ def run_adjoint(args) -> dict:
 
 
 def run_trajectories_bench(args) -> dict:
-    """Noisy 22-qubit GHZ, depolarizing p = 1e-3 after every gate on each touched
-    qubit, 1024 complex64 trajectories per batch, countsAll(64) each."""
+    """Noisy 22-qubit GHZ, a single-qubit channel after every gate on each touched
+    qubit, 1024 complex64 trajectories per batch, countsAll(64) each.  The default
+    channel is depolarizing p = 1e-3 (a Pauli mixture: branches drawn on the host,
+    applied inside the fused sweeps); ``--channel amplitude_damping`` uses amplitude
+    damping gamma = 1e-3 (state-dependent weights, each record weighed, drawn and
+    applied on the device).  ``value`` times whole batches through ``run_trajectories``
+    (the captured graph of the batch after the first call; outcomes and choices copied
+    back every step); ``kernel_stats`` and the roofline come from one more batch on a
+    context timing each kernel class."""
     from statecraft_b200 import _abi as A
+    from statecraft_b200 import noise as N
     from statecraft_b200 import workloads as W
     from statecraft_b200.engine import B200Config, NativeContext
     from statecraft_b200.trajectories import run_trajectories, touched_qubit_depolarizing
 
-    n, traj, shots = 22, args.trajectories, 64
+    n, traj, shots, p = 22, args.trajectories, 64, 1e-3
     c = W.ghz_circuit(n)
-    rec = touched_qubit_depolarizing(c, 1e-3)
-    ctx = NativeContext(B200Config(dtype=A.SC_C64, timing=True))
+    if args.channel == "amplitude_damping":
+        kraus = tuple(np.array(k.matrix, dtype=complex).reshape(2, 2)
+                      for k in N.AmplitudeDampingChannel(p, (0,)).krausDecomposition())
+        rec = [N.FlatChannel(i, q, kraus) for i, op in enumerate(c.operations)
+               for q in sorted(op.qubits_touched())]
+    else:
+        rec = touched_qubit_depolarizing(c, p)
+    ctx = NativeContext(B200Config(dtype=A.SC_C64, autotune=args.autotune))
     sec, r = _timed(lambda: run_trajectories(c, rec, traj, 2024, shots, 4096, context=ctx),
                     args.steps, args.warmup)
-    stats = {k: v for k, v in ctx.kernel_stats().items() if v["launches"]}
+    info = ctx.trajectories_info()
+    launches = {k: v["launches"] for k, v in ctx.kernel_stats().items() if v["launches"]}
     plan = ctx.plan_stats()
     ctx.close()
+    tctx = NativeContext(B200Config(dtype=A.SC_C64, timing=True, tile_qubits=info["tile_qubits"]))
+    run_trajectories(c, rec, traj, 2024, shots, 4096, context=tctx)
+    stats = {k: v for k, v in tctx.kernel_stats().items() if v["launches"]}
+    tctx.close()
     sw = stats.get("sweep", {"ms": 0.0, "bytes": 0.0, "launches": 0})
     peak = measured_peaks().get("hbm_gbs") or 6650.0
     gbs = sw["bytes"] / (sw["ms"] / 1e3) / 1e9 if sw["ms"] else None
     h = r.histogram()
     ghz = (h.get(0, 0) + h.get((1 << n) - 1, 0)) / (traj * shots)
-    return {"metric": f"trajectories/s (noisy GHZ 22q c64, touched-qubit depolarizing p=1e-3, "
+    chan = "amplitude damping gamma" if args.channel == "amplitude_damping" else "depolarizing p"
+    steps_launched = args.steps + args.warmup
+    return {"metric": f"trajectories/s (noisy GHZ 22q c64, touched-qubit {chan}=1e-3, "
                       f"{traj} trajectories x countsAll(64))",
             "value": traj / sec, "unit": "trajectories/s", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * sec, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": "noisy GHZ trajectories", "qubits": n, "trajectories": traj,
-                       "shots": shots, "p": 1e-3, "noise_seed": 2024, "measure_seed": 4096,
-                       "noise_records": len(rec), "sweeps": plan["sweeps"]},
+                       "shots": shots, "channel": args.channel, "p": p, "noise_seed": 2024,
+                       "measure_seed": 4096, "noise_records": len(rec),
+                       "sweeps": plan["sweeps"], "stages": plan["stages"],
+                       "tile_qubits": info["tile_qubits"], "nr": info["nr"],
+                       "graph": info["graph"], "autotune_ms": info["tuned_ms"]},
+            "gpu_launches": sum(launches.values()) // max(1, steps_launched),
             "kernel_stats": stats,
             "ghz_fraction": ghz,
             "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s",

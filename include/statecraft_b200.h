@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define SC_ABI_VERSION 1
+#define SC_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define SC_API __attribute__((visibility("default")))
@@ -100,6 +100,9 @@ typedef struct sc_config {
   int32_t timing;           /* 1 = record CUDA-event time per kernel class */
   int64_t device_mem_limit; /* bytes of device memory the context may allocate; 0 = no cap.
                                Exceeding it returns SC_ENOMEM without calling the allocator. */
+  int32_t autotune;         /* 1 = sc_trajectories times a few tile shapes on the first batch
+                               of a circuit and keeps the fastest (0 = the configured shape) */
+  int32_t reserved;
 } sc_config;
 
 #define SC_DEFAULT_MAX_QUBITS 32
@@ -192,17 +195,30 @@ SC_API int32_t sc_qaoa_batch_destroy(void* batch);
  * Runs n_traj (1..65535) copies of the circuit from |0..0> in the context's dtype;
  * trajectory t draws its Kraus branches from SplittableRandom(noise_seed + t), one
  * nextDouble(total) per noise record in record order, and samples `shots` outcomes
- * of all qubits from SplittableRandom(measure_seed + t).  Every record must be a
- * Pauli mixture (each Kraus operator a scalar times I, X, Y or Z: depolarizing,
- * bit flip, phase flip, ...); others return SC_EUNSUPPORTED.  Records are
- * sc_channel, sorted by after_op, e.g. one per touched qubit after each gate.
- * Outputs (caller-owned, any may be NULL): outcomes[t*shots + k] (basis index),
- * choices[t*n_channels + j] (chosen Kraus index), states[t * 2^(n+1) ...]
- * (interleaved doubles of every final state; small batches only). */
+ * of all qubits from SplittableRandom(measure_seed + t).  Records that are Pauli
+ * mixtures (each Kraus operator a scalar times I, X, Y or Z: depolarizing, bit flip,
+ * phase flip, ...) have state-independent weights: their branches are drawn on the
+ * host and applied inside the fused sweeps.  Any other record (amplitude or phase
+ * damping, thermal relaxation, ...) ends a fused segment: its branch weights
+ * ||K_k psi||^2 are summed on the device for every trajectory, the branch drawn
+ * there and K_k / sqrt(w_k) applied.  Invalid weights return SC_ESTATE (the
+ * reference's IllegalStateException).  Records are sc_channel, sorted by after_op,
+ * e.g. one per touched qubit after each gate.  Outputs (caller-owned, any may be
+ * NULL): outcomes[t*shots + k] (basis index), choices[t*n_channels + j] (chosen Kraus
+ * index), states[t * 2^(n+1) ...] (interleaved doubles of every final state; small
+ * batches only).  The context keeps the plans of its last batch and, unless
+ * cfg.timing is set, a CUDA graph of the batch's device work: a later call with the
+ * same circuit, records, n_traj, shots and configuration replays the graph (only the
+ * branch table and the seeds are uploaded). */
 SC_API int32_t sc_trajectories(void* ctx, int32_t n_qubits, const sc_op* ops, int64_t n_ops,
                                const sc_channel* channels, int64_t n_channels, int64_t n_traj,
                                uint64_t noise_seed, int64_t shots, uint64_t measure_seed,
                                int32_t* outcomes, int32_t* choices, double* states);
+/* The last trajectory batch of the context: tile qubits and register qubits it was
+ * planned with, 1 if a CUDA graph of it is held, and the time (ms) of the fastest
+ * shape when cfg.autotune chose it (0 otherwise).  Any pointer may be NULL. */
+SC_API int32_t sc_trajectories_info(void* ctx, int32_t* tile_qubits, int32_t* nr, int32_t* graph,
+                                    double* tuned_ms);
 
 /* Per-kernel-class device timing collected while cfg.timing = 1:
  * for class i in [0, cap): launches[i], milliseconds[i], bytes[i] (algorithmic

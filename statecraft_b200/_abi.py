@@ -10,7 +10,7 @@ import ctypes
 import os
 from pathlib import Path
 
-SC_ABI_VERSION = 1
+SC_ABI_VERSION = 2
 
 SC_OK = 0
 SC_EINVAL = -1
@@ -68,11 +68,13 @@ class ScConfig(ctypes.Structure):
         ("max_qubits", ctypes.c_int32),
         ("timing", ctypes.c_int32),
         ("device_mem_limit", ctypes.c_int64),
+        ("autotune", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 
 assert ctypes.sizeof(ScOp) == 280
-assert ctypes.sizeof(ScConfig) == 32
+assert ctypes.sizeof(ScConfig) == 40
 assert ctypes.sizeof(ScChannel) == 16 + 8 * 8 * SC_MAX_KRAUS
 
 
@@ -129,6 +131,9 @@ SIGNATURES = {
                                          ctypes.c_int64, ctypes.c_uint64, ctypes.c_int64,
                                          ctypes.c_uint64, _P(ctypes.c_int32),
                                          _P(ctypes.c_int32), _P(ctypes.c_double)]),
+    "sc_trajectories_info": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int32),
+                                              _P(ctypes.c_int32), _P(ctypes.c_int32),
+                                              _P(ctypes.c_double)]),
     "sc_kernel_stats": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int64),
                                          _P(ctypes.c_double), _P(ctypes.c_double),
                                          ctypes.c_int32]),

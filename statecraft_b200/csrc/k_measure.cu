@@ -23,7 +23,8 @@
 // array by a warp that splits them the same way into 32 segments and adds one by one
 // only inside the segments that cross -- and records the exact running sum before each
 // chunk, the exact total and the rescaling decision; when the reference rescales,
-// passes A-D run again on the rescaled probabilities.  Pass E gives each shot a warp
+// passes C and D run again on the rescaled probabilities (the running sums of pass B
+// times the scale classify their chunks).  Pass E gives each shot a warp
 // that binary-searches the exact chunk starts and replays its chunk: the exact start
 // of each lane's segment (lane effects and a warp scan), then exact FP64 adds within
 // each lane.
@@ -72,24 +73,20 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
 
 // pass A: sums[c] = sum of chunk c.  A batch of states of len_per entries each,
 // stored back to back, has chunks_per chunks per state (chunk c of the whole array is
-// chunk c % chunks_per of state c / chunks_per).  With `sc`, only the states the
-// reference rescales are summed, over their rescaled probabilities.
+// chunk c % chunks_per of state c / chunks_per).
 template <typename Src>
 __global__ void __launch_bounds__(kThreadsA) k_chunk_sums(Src src, uint64_t len_per,
                                                           uint64_t chunks_per, double* sums,
-                                                          uint64_t chunks,
-                                                          const SampleScalars* sc) {
+                                                          uint64_t chunks) {
   __shared__ double red[kThreadsA / 32];
   for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
     const uint64_t st = c / chunks_per;
-    if (sc && !sc[st].scaled) continue;
-    const double scale = sc ? sc[st].scale : 1.0;
     const uint64_t b = (c - st * chunks_per) * kChunk;
     const uint64_t off = st * len_per;
     double acc = 0.0;
     for (int k = threadIdx.x; k < kChunk; k += kThreadsA) {
       const uint64_t i = b + k;
-      if (i < len_per) acc += sc ? __dmul_rn(src(off + i), scale) : src(off + i);
+      if (i < len_per) acc += src(off + i);
     }
     const double s = block_sum<kThreadsA>(acc, red);
     if (threadIdx.x == 0) sums[c] = s;
@@ -99,8 +96,7 @@ __global__ void __launch_bounds__(kThreadsA) k_chunk_sums(Src src, uint64_t len_
 // pass B (one CTA of 1024 threads per state): approximate exclusive running sums of
 // the chunk sums
 __global__ void __launch_bounds__(1024) k_prefix_approx(const double* sums, uint64_t chunks,
-                                                        double* prefix, const SampleScalars* sc) {
-  if (sc && !sc[blockIdx.x].scaled) return;
+                                                        double* prefix) {
   sums += blockIdx.x * chunks;
   prefix += blockIdx.x * chunks;
   __shared__ double part[1024];
@@ -347,7 +343,9 @@ __global__ void __launch_bounds__(kThreadsA) k_chunk_tf(Src src, uint64_t len_pe
       bool clean = cl + 1 < chunks_per;
       int e = -2000;
       if (clean) {
-        const double a = prefix[c], b = prefix[c + 1];
+        // on the rescaled pass the running sums of the unscaled probabilities times the
+        // scale stand in for those of the scaled ones (relative error ~2^-52 per value)
+        const double a = prefix[c] * scale, b = prefix[c + 1] * scale;
         e = binade(a * (1.0 - kMargin));
         clean = e > -1000 && binade(a) == e && binade(b * (1.0 + kMargin)) == e;
       }
@@ -530,9 +528,11 @@ __global__ void __launch_bounds__(256) k_sample_shots(Src src_all, uint64_t len,
                                                       const ChunkTf* tfs_all, uint64_t chunks,
                                                       const SampleScalars* sc,
                                                       const double* uniforms, uint64_t seed,
+                                                      const uint64_t* seed_dev,
                                                       int64_t shots_per, int64_t shots_total,
                                                       int32_t* out) {
   const int lane = threadIdx.x & 31;
+  if (seed_dev) seed = *seed_dev;
   const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
   const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t g = warp; g < shots_total; g += nwarps) {
@@ -704,10 +704,11 @@ cudaError_t sample_src(Src src, uint64_t len, int64_t batch, const SampleArgs& a
   // the running sum of the probabilities, then (decided on the device, per state) of
   // the rescaled probabilities when the reference rescales
   for (int pass = 0; pass < 2; ++pass) {
-    const SampleScalars* gate = pass ? a.scalars : nullptr;
-    k_chunk_sums<Src><<<grid_chunks, kThreadsA, 0, s>>>(src, len, chunks, a.chunk_sums,
-                                                        all_chunks, gate);
-    k_prefix_approx<<<(unsigned)batch, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix, gate);
+    if (pass == 0) {
+      k_chunk_sums<Src><<<grid_chunks, kThreadsA, 0, s>>>(src, len, chunks, a.chunk_sums,
+                                                          all_chunks);
+      k_prefix_approx<<<(unsigned)batch, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix);
+    }
     k_chunk_tf<Src><<<grid_chunks, kThreadsA, 0, s>>>(src, len, chunks, all_chunks,
                                                       a.chunk_prefix, a.scalars, pass == 1,
                                                       a.chunk_tf);
@@ -718,7 +719,7 @@ cudaError_t sample_src(Src src, uint64_t len, int64_t batch, const SampleArgs& a
     const int64_t total = a.shots * batch;
     const int blocks = grid_cap((uint64_t)total * 32, 256, a.sm_count);
     k_sample_shots<Src><<<blocks, 256, 0, s>>>(src, len, a.chunk_start, a.chunk_tf, chunks,
-                                               a.scalars, a.uniforms, a.seed, a.shots, total,
+                                               a.scalars, a.uniforms, a.seed, a.seed_dev, a.shots, total,
                                                a.outcomes);
   }
   return cudaGetLastError();

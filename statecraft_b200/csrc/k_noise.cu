@@ -8,6 +8,7 @@
 // uniform from the noise SplitMix64 stream and writes K_i / sqrt(w_i) (the norm
 // after applying K_i is w_i) to device memory, and one read-write sweep applies
 // it.  Two sweeps per channel application instead of seven, and no host round trip.
+#include <algorithm>
 #include <cfloat>
 
 #include "sc_device.cuh"
@@ -19,6 +20,7 @@ namespace sc {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kUnroll = 4;  // amplitude pairs in flight per thread (batched kernels)
 
 template <typename R>
 __global__ void __launch_bounds__(kThreads)
@@ -127,7 +129,185 @@ __global__ void k_kraus_apply(typename Amp<R>::type* __restrict__ st, int n, int
   }
 }
 
+// ---- batches of trajectories: the same three steps for every state at once --------
+// States of 2^n amplitudes back to back; blockIdx.y is the state, blockIdx.x a slice
+// of its amplitude pairs.
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+    k_kraus_weights_batch(const typename Amp<R>::type* __restrict__ states, int n, KrausArgs a,
+                          const int32_t* __restrict__ status, double* __restrict__ partial) {
+  __shared__ double red[kThreads / 32][SC_MAX_KRAUS];
+  const uint64_t t = blockIdx.y;
+  const typename Amp<R>::type* st = states + (t << n);
+  double w[SC_MAX_KRAUS];
+#pragma unroll
+  for (int k = 0; k < SC_MAX_KRAUS; ++k) w[k] = 0.0;
+  const uint64_t pairs = 1ULL << (n - 1);
+  const uint64_t stride = 1ULL << a.target;
+  if (status[t] == 0) {
+    // kUnrollW pairs per thread and step, their loads issued together
+    constexpr int kUnrollW = 2;
+    const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t p0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p0 < pairs;
+         p0 += kUnrollW * step) {
+      typename Amp<R>::type v0[kUnrollW], v1[kUnrollW];
+#pragma unroll
+      for (int u = 0; u < kUnrollW; ++u) {
+        const uint64_t p = p0 + u * step;
+        if (p < pairs) {
+          const uint64_t i0 = insert_zero64(p, a.target);
+          v0[u] = st[i0];
+          v1[u] = st[i0 + stride];
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnrollW; ++u) {
+        if (p0 + u * step >= pairs) break;
+        const double a0r = v0[u].x, a0i = v0[u].y, a1r = v1[u].x, a1i = v1[u].y;
+#pragma unroll
+        for (int k = 0; k < SC_MAX_KRAUS; ++k) {
+          if (k >= a.nk) break;
+          const double* K = a.k[k];
+          const double o0r = K[0] * a0r - K[1] * a0i + K[2] * a1r - K[3] * a1i;
+          const double o0i = K[0] * a0i + K[1] * a0r + K[2] * a1i + K[3] * a1r;
+          const double o1r = K[4] * a0r - K[5] * a0i + K[6] * a1r - K[7] * a1i;
+          const double o1i = K[4] * a0i + K[5] * a0r + K[6] * a1i + K[7] * a1r;
+          w[k] += (o0r * o0r + o0i * o0i) + (o1r * o1r + o1i * o1i);
+        }
+      }
+    }
+  }
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int k = 0; k < SC_MAX_KRAUS; ++k) {
+    double v = w[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[wid][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < SC_MAX_KRAUS) {
+    double sum = 0.0;
+    for (int q = 0; q < kThreads / 32; ++q) sum += red[q][threadIdx.x];
+    partial[(t * gridDim.x + blockIdx.x) * SC_MAX_KRAUS + threadIdx.x] = sum;
+  }
+}
+
+// one thread per trajectory: the weights summed in a fixed order, validated, the
+// branch drawn from SplittableRandom(seeds[0] + t) (draw number `draw`) and K / sqrt(w)
+// written to mats[t]; status[t] records the first failure of trajectory t
+__global__ void k_kraus_select_batch(const double* __restrict__ partial, int nblocks,
+                                     KrausArgs a, const uint64_t* __restrict__ seeds,
+                                     uint64_t draw, int64_t batch, double* __restrict__ mats,
+                                     int32_t* __restrict__ choices, int64_t choice_stride,
+                                     int32_t* __restrict__ status) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= batch || status[t] != 0) return;
+  double w[SC_MAX_KRAUS];
+  double total = 0.0;
+  for (int k = 0; k < a.nk; ++k) {
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partial[((uint64_t)t * nblocks + b) * SC_MAX_KRAUS + k];
+    if (!isfinite(s) || s < 0.0) {
+      status[t] = kNoiseBadWeight;
+      return;
+    }
+    w[k] = s;
+    total += s;
+  }
+  if (!isfinite(total) || total <= 1e-15) {
+    status[t] = kNoiseBadTotal;
+    return;
+  }
+  double u = splitmix_double(seeds[0] + (uint64_t)t, draw) * total;
+  if (u >= total) u = nextafter(total, -DBL_MAX);
+  int idx = a.nk - 1;
+  double cum = 0.0;
+  for (int k = 0; k < a.nk; ++k) {
+    cum += w[k];
+    if (u < cum) {
+      idx = k;
+      break;
+    }
+  }
+  const double nsq = w[idx];
+  if (!isfinite(nsq) || nsq == 0.0) {
+    status[t] = kNoiseBadNorm;
+    return;
+  }
+  const double scale = (fabs(nsq - 1.0) > 1e-12) ? 1.0 / sqrt(nsq) : 1.0;
+  for (int e = 0; e < 8; ++e) mats[t * 8 + e] = a.k[idx][e] * scale;
+  choices[t * choice_stride] = idx;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(kThreads)
+    k_kraus_apply_batch(typename Amp<R>::type* __restrict__ states, int n, int target,
+                        const double* __restrict__ mats, const int32_t* __restrict__ status) {
+  const uint64_t t = blockIdx.y;
+  if (status[t] != 0) return;
+  typename Amp<R>::type* st = states + (t << n);
+  const double* m = mats + t * 8;
+  const R m00r = (R)m[0], m00i = (R)m[1], m01r = (R)m[2], m01i = (R)m[3];
+  const R m10r = (R)m[4], m10i = (R)m[5], m11r = (R)m[6], m11i = (R)m[7];
+  const uint64_t pairs = 1ULL << (n - 1);
+  const uint64_t stride = 1ULL << target;
+  const uint64_t step = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t p0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p0 < pairs;
+       p0 += kUnroll * step) {
+    typename Amp<R>::type a0[kUnroll], a1[kUnroll];
+    uint64_t i0[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      const uint64_t p = p0 + u * step;
+      i0[u] = insert_zero64(p < pairs ? p : 0, target);
+      if (p < pairs) {
+        a0[u] = st[i0[u]];
+        a1[u] = st[i0[u] + stride];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (p0 + u * step >= pairs) break;
+      st[i0[u]] = cmac2(m00r, m00i, a0[u], m01r, m01i, a1[u]);
+      st[i0[u] + stride] = cmac2(m10r, m10i, a0[u], m11r, m11i, a1[u]);
+    }
+  }
+}
+
 }  // namespace
+
+int noise_grid_batch(int n, int64_t batch, int sm_count) {
+  const uint64_t pairs = 1ULL << (n - 1);
+  const uint64_t most = (pairs + kThreads - 1) / kThreads;
+  const uint64_t want = ((uint64_t)sm_count * 8 + (uint64_t)batch - 1) / (uint64_t)batch;
+  return (int)std::max<uint64_t>(1, std::min(most, want));
+}
+
+cudaError_t launch_kraus_batch(int dtype, void* states, int n, int64_t batch, const KrausArgs& a,
+                               const uint64_t* seeds, uint64_t draw, double* partial,
+                               double* mats, int32_t* choices, int64_t choice_stride,
+                               int32_t* status, int sm_count, cudaStream_t s) {
+  if (batch < 1 || batch > 65535 || n < 1) return cudaErrorInvalidValue;
+  const int gx = noise_grid_batch(n, batch, sm_count);
+  const dim3 grid((unsigned)gx, (unsigned)batch);
+  if (dtype == SC_C64)
+    k_kraus_weights_batch<float><<<grid, kThreads, 0, s>>>(static_cast<const float2*>(states), n,
+                                                           a, status, partial);
+  else
+    k_kraus_weights_batch<double><<<grid, kThreads, 0, s>>>(static_cast<const double2*>(states),
+                                                            n, a, status, partial);
+  k_kraus_select_batch<<<(unsigned)((batch + 127) / 128), 128, 0, s>>>(
+      partial, gx, a, seeds, draw, batch, mats, choices, choice_stride, status);
+  if (dtype == SC_C64)
+    k_kraus_apply_batch<float><<<grid, kThreads, 0, s>>>(static_cast<float2*>(states), n,
+                                                         a.target, mats, status);
+  else
+    k_kraus_apply_batch<double><<<grid, kThreads, 0, s>>>(static_cast<double2*>(states), n,
+                                                          a.target, mats, status);
+  return cudaGetLastError();
+}
 
 int noise_grid(int n, int sm_count) {
   const uint64_t pairs = 1ULL << (n - 1);

@@ -533,6 +533,8 @@ int32_t sc_destroy(void* p) {
   cudaStreamSynchronize(c->stream);
   for (void* b : c->qaoa_batches) qaoa_batch_free(b);
   c->qaoa_batches.clear();
+  traj_cache_free(c->traj_cache);
+  c->traj_cache = nullptr;
   c->release_all();
   for (cudaEvent_t ev : c->event_pool) cudaEventDestroy(ev);
   cudaStreamDestroy(c->stream);

@@ -16,6 +16,8 @@ int fail(int code, const char* fmt, ...);
 int fail_cuda(cudaError_t e, const char* where);
 // frees a QAOA batch (sc_qaoa.cpp) and its device buffers
 void qaoa_batch_free(void* batch);
+// frees the cached trajectory batch (plans and CUDA graph, sc_trajectories.cpp)
+void traj_cache_free(void* cache);
 // context handle check (also makes its device current) and the op / noise-record
 // validation of sc_run, shared with the batched entry points
 int check_context(void* ctx);
@@ -76,6 +78,8 @@ struct Ctx {
 
   // QAOA batches created on this context (freed by sc_destroy)
   std::vector<void*> qaoa_batches;
+  // the last trajectory batch: its plans and captured graph (freed by sc_destroy)
+  void* traj_cache = nullptr;
 
   // plan statistics of the last run
   int64_t plan_sweeps_count = 0, plan_gates = 0, plan_stages = 0, plan_blocks = 0;

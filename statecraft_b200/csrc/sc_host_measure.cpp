@@ -84,7 +84,7 @@ int Ctx::sample(const int32_t* qubits, int32_t m, int64_t shots, uint64_t seed,
                         cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return fail_cuda(e, "uniform upload");
   }
-  mark_begin(KC_SAMPLE, (direct ? dim * amp_bytes : 8.0 * (double)len), 3);
+  mark_begin(KC_SAMPLE, (direct ? dim * amp_bytes : 8.0 * (double)len), kSampleKernels);
   e = launch_sample(cfg.dtype, state.p, probs, len, a, stream);
   mark_end();
   if (e != cudaSuccess) return fail_cuda(e, "sampling kernels");

@@ -36,12 +36,17 @@ struct SampleArgs {
   SampleScalars* scalars;  // device, one per state
   const double* uniforms;  // device or nullptr (then SplitMix64(seed))
   uint64_t seed;
+  const uint64_t* seed_dev = nullptr;  // device copy of the seed, read instead of `seed`
   int64_t shots;         // 0: only the prefix sums
   int32_t* outcomes;     // device, shots entries
   int sm_count;
 };
 
 uint64_t sample_chunks(uint64_t len);
+// kernels one launch_sample / launch_sample_batch enqueues (chunk sums, running sums,
+// chunk effects and exact starts; effects and exact starts again for the rescaled
+// probabilities; the per-shot search)
+constexpr int kSampleKernels = 7;
 
 // probs[o] = marginal probability of outcome o over the measured mask (m bits).
 // scratch must hold 2^m * ceil(2^(n-m) / kSampleChunk) doubles when 2^(n-m) > 64.

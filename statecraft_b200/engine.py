@@ -301,6 +301,7 @@ class B200Config:
     max_qubits: int = 0
     timing: bool = False
     device_mem_limit: int = 0
+    autotune: bool = False
 
     def to_native(self) -> A.ScConfig:
         cfg = A.ScConfig()
@@ -311,6 +312,7 @@ class B200Config:
         cfg.max_qubits = self.max_qubits
         cfg.timing = 1 if self.timing else 0
         cfg.device_mem_limit = self.device_mem_limit
+        cfg.autotune = 1 if self.autotune else 0
         return cfg
 
 
@@ -418,6 +420,14 @@ class NativeContext:
 
     def reset_kernel_stats(self) -> None:
         self._check(self.lib.sc_reset_kernel_stats(self.handle))
+
+    def trajectories_info(self) -> dict:
+        """Shape, graph and tuning time of the context's last trajectory batch."""
+        t, r, g = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        ms = ctypes.c_double()
+        self._check(self.lib.sc_trajectories_info(self.handle, ctypes.byref(t), ctypes.byref(r),
+                                                  ctypes.byref(g), ctypes.byref(ms)))
+        return {"tile_qubits": t.value, "nr": r.value, "graph": g.value, "tuned_ms": ms.value}
 
     def plan_stats(self) -> dict:
         s, g, st = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

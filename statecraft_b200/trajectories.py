@@ -3,10 +3,15 @@
 The reference engine samples one Monte-Carlo trajectory per ``simulate`` call
 (StatevectorEngine.java:371-600); a study over many trajectories runs the call in a
 loop, trajectory t with noise seed S + t (StatecraftComparisonRunner.java:75).  Here
-all trajectories of a circuit with Pauli-mixture noise (depolarizing, bit / phase
-flip) run as one batch: each trajectory draws its branches from the same
-SplittableRandom stream the reference would use, and each sweep of the fused plan
-is one kernel launch over every trajectory's state.
+all trajectories of a circuit run as one batch: each trajectory draws its branches
+from the same SplittableRandom stream the reference would use, and each sweep of the
+fused plan is one kernel launch over every trajectory's state.  Pauli-mixture
+records (depolarizing, phase flip) are drawn on the host and applied inside the
+sweeps; records with state-dependent weights (amplitude / phase damping, thermal
+relaxation) split the plan and are weighed, drawn and applied on the device for all
+trajectories at once.  A repeated call with the same circuit and records replays a
+captured CUDA graph (``NativeContext.trajectories_info``); ``B200Config(autotune=True)``
+times a few tile shapes on the first batch and keeps the fastest.
 """
 from __future__ import annotations
 

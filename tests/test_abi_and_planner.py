@@ -36,7 +36,7 @@ def test_abi_version_and_struct_sizes():
     assert lib.sc_version() == A.SC_ABI_VERSION
     assert ctypes.sizeof(A.ScOp) == 280
     assert ctypes.sizeof(A.ScChannel) == 528
-    assert ctypes.sizeof(A.ScConfig) == 32
+    assert ctypes.sizeof(A.ScConfig) == 40
 
 
 def test_create_without_gpu_fails_cleanly():

@@ -137,10 +137,118 @@ def test_histograms_match_oracle(ctx):
     assert total_variation(h_gpu, h_or) <= max(0.01, 3 * total_variation(h_or, h_other))
 
 
-def test_non_pauli_channel_rejected(ctx):
-    c = W.ghz_circuit(4)
-    ad = N.AmplitudeDampingChannel(0.1, (0,))
-    kraus = tuple(np.array(k.matrix, dtype=complex).reshape(2, 2) for k in ad.krausDecomposition())
-    rec = [N.FlatChannel(0, 0, kraus)]
-    with pytest.raises(A.UnsupportedOperationException):
-        run_trajectories(c, rec, 4, noise_seed=1, shots=8, measure_seed=1, context=ctx)
+def _channel_records(circuit, channels):
+    """channels[k % len] after gate k, on every qubit the gate touches"""
+    out = []
+    from statecraft_b200 import quantum as Q
+    for i, op in enumerate(circuit.operations):
+        if isinstance(op, Q.MeasureOperation):
+            continue
+        chan = channels[i % len(channels)]
+        if chan is None:
+            continue
+        kraus = tuple(np.array(k.matrix, dtype=complex).reshape(2, 2)
+                      for k in chan.krausDecomposition())
+        for q in sorted(op.qubits_touched()):
+            out.append(N.FlatChannel(i, q, kraus))
+    return out
+
+
+_CHANNELS = {
+    "amplitude_damping": [N.AmplitudeDampingChannel(0.2, (0,))],
+    "phase_damping": [N.PhaseDampingChannel(0.3, (0,))],
+    "thermal": [N.ThermalRelaxationChannel(50.0, 70.0, 9.0, (0,))],
+    "mixed": [N.AmplitudeDampingChannel(0.15, (0,)), N.DepolarizingChannel(0.2, (0,)), None,
+              N.PhaseDampingChannel(0.25, (0,)), N.PhaseFlipChannel(0.3, (0,))],
+}
+
+
+@pytest.mark.parametrize("kind", sorted(_CHANNELS))
+def test_state_dependent_channels_match_oracle(ctx, kind):
+    # records whose branch weights depend on the state end a fused segment; their
+    # weights, draws and K / sqrt(w) run on the device for every trajectory
+    n, traj = 9, 12
+    c = RCirc.random_circuit(n, 40, seed=910)
+    rec = _channel_records(c, _CHANNELS[kind])
+    res = run_trajectories(c, rec, traj, noise_seed=313, shots=0, measure_seed=0,
+                           return_states=True, context=ctx)
+    for t in range(traj):
+        want, chosen = _oracle_trajectory(c, rec, 313 + t)
+        np.testing.assert_array_equal(res.choices[t], chosen)
+        np.testing.assert_allclose(res.states[t], want, rtol=0, atol=1e-12)
+    assert np.count_nonzero(res.choices) > 0
+
+
+def test_state_dependent_channels_complex64(ctx64):
+    c = W.ghz_circuit(10)
+    rec = _channel_records(c, [N.AmplitudeDampingChannel(0.3, (0,))])
+    res = run_trajectories(c, rec, 8, noise_seed=21, shots=0, measure_seed=0,
+                           return_states=True, context=ctx64)
+    for t in range(8):
+        want, chosen = _oracle_trajectory(c, rec, 21 + t)
+        np.testing.assert_array_equal(res.choices[t], chosen)
+        np.testing.assert_allclose(res.states[t], want, rtol=0, atol=2e-5)
+
+
+def test_graph_replay_and_seeds(ctx):
+    # the second call with the same circuit replays the captured graph; new seeds
+    # reach its kernels through device memory; a timed (eager) context agrees
+    n, traj, shots = 11, 40, 32
+    c = W.ghz_circuit(n)
+    rec = _channel_records(c, [N.AmplitudeDampingChannel(0.1, (0,)), N.DepolarizingChannel(0.05, (0,))])
+    a = run_trajectories(c, rec, traj, noise_seed=5, shots=shots, measure_seed=6, context=ctx)
+    info = ctx.trajectories_info()
+    assert info["graph"] == 1
+    b = run_trajectories(c, rec, traj, noise_seed=5, shots=shots, measure_seed=6, context=ctx)
+    np.testing.assert_array_equal(a.outcomes, b.outcomes)
+    np.testing.assert_array_equal(a.choices, b.choices)
+    d = run_trajectories(c, rec, traj, noise_seed=500, shots=shots, measure_seed=600,
+                         return_states=True, context=ctx)
+    for t in range(0, traj, 7):
+        want, chosen = _oracle_trajectory(c, rec, 500 + t)
+        np.testing.assert_array_equal(d.choices[t], chosen)
+        np.testing.assert_allclose(d.states[t], want, rtol=0, atol=1e-12)
+    timed = NativeContext(B200Config(timing=True))
+    try:
+        e = run_trajectories(c, rec, traj, noise_seed=5, shots=shots, measure_seed=6, context=timed)
+        assert timed.trajectories_info()["graph"] == 0
+    finally:
+        timed.close()
+    np.testing.assert_array_equal(a.outcomes, e.outcomes)
+    np.testing.assert_array_equal(a.choices, e.choices)
+
+
+def test_autotuned_shape_matches_oracle():
+    tuned = NativeContext(B200Config(autotune=True))
+    try:
+        n = 14
+        c = RCirc.random_circuit(n, 50, seed=14)
+        rec = touched_qubit_depolarizing(c, 0.05)
+        res = run_trajectories(c, rec, 6, noise_seed=9, shots=0, measure_seed=0,
+                               return_states=True, context=tuned)
+        info = tuned.trajectories_info()
+        assert info["tuned_ms"] > 0.0 and info["tile_qubits"] > 0
+        for t in range(6):
+            want, chosen = _oracle_trajectory(c, rec, 9 + t)
+            np.testing.assert_array_equal(res.choices[t], chosen)
+            np.testing.assert_allclose(res.states[t], want, rtol=0, atol=1e-12)
+    finally:
+        tuned.close()
+
+
+def test_invalid_weights_raise_illegal_state(ctx):
+    from statecraft_b200 import quantum as Q
+
+    c = Q.QuantumCircuit(4).append(Q.PauliZ(), 1)
+    # a Pauli record with zero weight (the host draw) and a projector onto |1> of a
+    # qubit in |0> (weights summed on the device, total 0): both IllegalStateException
+    zero = (np.zeros((2, 2), dtype=complex),)
+    proj = (np.array([[0, 0], [0, 1]], dtype=complex),)
+    for kraus in (zero, proj):
+        with pytest.raises(A.IllegalStateException):
+            run_trajectories(c, [N.FlatChannel(0, 0, kraus)], 4, noise_seed=1, shots=8,
+                             measure_seed=1, context=ctx)
+    # the context still runs batches
+    ok = run_trajectories(W.ghz_circuit(4), [], 2, noise_seed=1, shots=4, measure_seed=1,
+                          context=ctx)
+    assert set(np.unique(ok.outcomes)) <= {0, 15}
