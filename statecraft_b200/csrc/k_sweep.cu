@@ -778,6 +778,13 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
 #undef SC_DO_XF
 #undef SC_DO_CXF
           SC_CASES_1(SK_PAULI, SC_DO_PAULI)
+#define SC_DO_TMAT(A)                                                                     \
+  if constexpr (kBatch) {                                                                 \
+    g1<R, NR, A>(v, p.tmats + ((uint64_t)g.b * (uint64_t)p.batch + (t >> p.tiles_log2)) * 8, \
+                 l0, off, 0u);                                                            \
+  }
+          SC_CASES_1(SK_TMAT, SC_DO_TMAT)
+#undef SC_DO_TMAT
           case SK_PAULIF << 4:
             if constexpr (kBatch) {
               pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
@@ -1271,7 +1278,7 @@ cudaError_t launch_nr(void* state, const SweepParams<R>& p, int* err, int sm_cou
 
 template <typename R, int NR>
 cudaError_t launch_pick(void* state, SweepParams<R>& p, int* err, int sm_count, cudaStream_t s) {
-  const bool batch = p.batch > 1 || p.n_local_slots > 0;
+  const bool batch = p.batch > 1 || p.n_local_slots > 0 || p.tmats != nullptr;
   p.stall_first = 0;
   if (const char* v = getenv("STATECRAFT_B200_TEST_STALL_CYCLES")) p.stall_first = atoi(v);
   if (make_tile_tensor<R>(state, p))
@@ -1432,6 +1439,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
   p->pad2 = 0;
   p->batch = 1;
   p->paulis = nullptr;
+  p->tmats = nullptr;
   p->n_local_slots = 0;
   for (int q = 0; q < SW_MAX_HIGH; ++q) {
     p->hq[q] = sw.hq[q];
@@ -1667,8 +1675,8 @@ cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int
 }
 
 cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, const Plan& plan,
-                               size_t k, const uint8_t* paulis, int n_slots, int* err,
-                               int sm_count, cudaStream_t s) {
+                               size_t k, const uint8_t* paulis, int n_slots, const void* tmats,
+                               int* err, int sm_count, cudaStream_t s) {
   if (batch < 1 || ((uint64_t)plan.sweeps[k].tiles * (uint64_t)batch) > 0xffffffffull)
     return cudaErrorInvalidValue;
   auto fill = [&](auto* p) {
@@ -1677,6 +1685,7 @@ cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, co
     p->batch = batch;
     p->paulis = paulis;
     p->n_slots = n_slots;
+    p->tmats = static_cast<const typename std::remove_pointer<decltype(p->tmats)>::type*>(tmats);
     return true;
   };
   if (dtype == SC_C64) {

@@ -18,7 +18,8 @@ static inline bool czero(double re, double im) { return re == 0.0 && im == 0.0; 
 
 double gate_cost(const PGate& g) {
   switch (g.kind) {
-    case PK_DENSE1: return 8.0;   // 2 complex MACs per amplitude
+    case PK_DENSE1:
+    case PK_TMAT: return 8.0;     // 2 complex MACs per amplitude
     case PK_DENSE2: return 16.0;  // 4 complex MACs per amplitude
     case PK_DIAG1:
     case PK_DIAG2: return 3.0;    // 1 complex multiply + bit tests
@@ -44,6 +45,7 @@ uint64_t dense_mask(const PGate& g) {
     case PK_DENSE1:
     case PK_PAULI:
     case PK_PROBE:
+    case PK_TMAT:
     case PK_X: return 1ULL << g.q0;
     case PK_DENSE2:
     case PK_SWAP: return (1ULL << g.q0) | (1ULL << g.q1);
@@ -52,7 +54,7 @@ uint64_t dense_mask(const PGate& g) {
 }
 
 uint64_t touch_mask(const PGate& g) {
-  if (g.kind == PK_PAULI) return 1ULL << g.q0;
+  if (g.kind == PK_PAULI || g.kind == PK_TMAT) return 1ULL << g.q0;
   uint64_t m = g.cmask | (1ULL << g.q0);
   if (g.kind == PK_DENSE2 || g.kind == PK_SWAP || g.kind == PK_DIAG2) m |= 1ULL << g.q1;
   return m;
@@ -268,7 +270,9 @@ uint32_t record_bits(const SwGate& g, const int* reg_of_pos) {
     if (p >= 0 && p < 32 && reg_of_pos[p] >= 0) f |= 1u << reg_of_pos[p];
   };
   switch (g.kind) {
-    case SK_G1: case SK_X: case SK_X0: case SK_D1R: case SK_PAULI: case SK_XF: f |= 1u << g.a; break;
+    case SK_G1: case SK_X: case SK_X0: case SK_D1R: case SK_PAULI: case SK_XF: case SK_TMAT:
+      f |= 1u << g.a;
+      break;
     case SK_G2: case SK_CX: case SK_CX0: case SK_DPR: case SK_SWAP: case SK_CXF:
       f |= (1u << g.a) | (1u << g.b);
       break;
@@ -1100,6 +1104,11 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             sg.kind = SK_PAULI;
             sg.a = reg_of_pos[pos_of[pg.q0]];
             sg.b = pg.q1;  // slot
+            break;
+          case PK_TMAT:
+            sg.kind = SK_TMAT;
+            sg.a = reg_of_pos[pos_of[pg.q0]];
+            sg.b = pg.q1;  // Kraus point
             break;
           case PK_PROBE:
             sg.kind = SK_PROBE;

@@ -25,8 +25,11 @@ namespace sc {
 //              is chosen per trajectory; q1 = slot index into the choice table
 // PK_PROBE (adjoint reverse pass only): q0 = qubit, q1 = Pauli generator (1 = X,
 // 2 = Y, 3 = Z), op_index = gradient slot; adds Im <lambda| P |psi> to that slot.
+// PK_TMAT (batched trajectories): a 2x2 matrix on q0 chosen per trajectory on the
+// device (a drawn Kraus operator over the square root of its weight); q1 = its
+// index among the batch's Kraus points.
 enum PKind : int32_t {
-  PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2, PK_PAULI, PK_PROBE
+  PK_DENSE1 = 0, PK_DENSE2, PK_X, PK_SWAP, PK_DIAG1, PK_DIAG2, PK_PAULI, PK_PROBE, PK_TMAT
 };
 
 struct PGate {
@@ -88,9 +91,11 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 // SK_DTAB: a diagonal over the stage's register bits as a table of 2^NR complex
 //        factors (register j is multiplied by entry j): adjacent register-bit
 //        diagonals of a stage merged into one record.
+// SK_TMAT: 2x2 matrix on register bit a read per trajectory from the batch's matrix
+//        table (b = Kraus point: entry b * batch + trajectory, 8 reals).
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF, SK_DTAB
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF, SK_DTAB, SK_TMAT
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
@@ -98,7 +103,7 @@ enum SwKind : int32_t {
 // kernel switches on it once.
 inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
   switch (kind) {
-    case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: case SK_XF:
+    case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: case SK_XF: case SK_TMAT:
       return (kind << 4) | (a << 2);
     case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0: case SK_CXF:
       return (kind << 4) | (a << 2) | b;
@@ -232,10 +237,11 @@ cudaError_t launch_gate(int dtype, void* state, int n, const PGate& g, cudaStrea
 cudaError_t launch_sweep(int dtype, void* state, const Plan& plan, size_t k, int* err,
                          int sm_count, cudaStream_t s);
 // the same sweep over `batch` states of n qubits stored back to back; Pauli slots
-// read trajectory b's choice of slot j at paulis[b * n_slots + j]
+// read trajectory b's choice of slot j at paulis[b * n_slots + j]; SK_TMAT records
+// read their matrix at tmats + (point * batch + b) * 8 (float or double per dtype)
 cudaError_t launch_sweep_batch(int dtype, void* states, int n, int64_t batch, const Plan& plan,
-                               size_t k, const uint8_t* paulis, int n_slots, int* err,
-                               int sm_count, cudaStream_t s);
+                               size_t k, const uint8_t* paulis, int n_slots, const void* tmats,
+                               int* err, int sm_count, cudaStream_t s);
 // Fused adjoint reverse pass (plans of inverse gates with SK_PROBE records):
 // adjoint_plan_supported says whether every sweep fits the dual-state kernel
 // (register qubits 3, at least 32 threads per tile, matrix / permutation /

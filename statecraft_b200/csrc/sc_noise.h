@@ -37,16 +37,20 @@ cudaError_t launch_kraus_channel(int dtype, void* state, int n, const KrausArgs&
                                  uint64_t seed, uint64_t draw, double* partial,
                                  NoiseDevState* ns, int sm_count, cudaStream_t s);
 
-// The same for `batch` states of n qubits stored back to back (trajectory t draws
-// from SplittableRandom(seeds[0] + t), seeds in device memory): partial holds
-// batch * noise_grid_batch(n, batch) * SC_MAX_KRAUS doubles, mats 8 doubles per state;
-// the chosen index of state t goes to choices[t * choice_stride]; a state whose
-// status is nonzero is skipped, and a failed draw sets it (kNoiseBad*).
+// Weights and draw of one Kraus point for `batch` states of n qubits stored back to
+// back (trajectory t draws from SplittableRandom(seeds[0] + t), seeds in device
+// memory).  K_k / sqrt(w_k) of state t goes to mats + t * 8 (reals of the dtype) for
+// the next sweep to apply; with `pend`, state t's matrix pend + t * 8 on qubit pend_q
+// (not yet applied) is applied before weighing.  partial holds batch *
+// noise_grid_batch(n, batch) * SC_MAX_KRAUS doubles; the chosen index of state t goes
+// to choices[t * choice_stride]; a state whose status is nonzero is skipped, and a
+// failed draw sets it (kNoiseBad*).
 int noise_grid_batch(int n, int64_t batch, int sm_count);
-cudaError_t launch_kraus_batch(int dtype, void* states, int n, int64_t batch, const KrausArgs& a,
-                               const uint64_t* seeds, uint64_t draw, double* partial,
-                               double* mats, int32_t* choices, int64_t choice_stride,
-                               int32_t* status, int sm_count, cudaStream_t s);
+cudaError_t launch_kraus_batch(int dtype, const void* states, int n, int64_t batch,
+                               const KrausArgs& a, int pend_q, const void* pend,
+                               const uint64_t* seeds, uint64_t draw, double* partial, void* mats,
+                               int32_t* choices, int64_t choice_stride, int32_t* status,
+                               int sm_count, cudaStream_t s);
 
 // Pauli-sum expectation: out_partial[t] receives term t's <psi|P_t|psi> (real part).
 cudaError_t launch_pauli_terms(int dtype, const void* state, int n, int n_terms,

@@ -63,6 +63,7 @@ struct SweepParams {
   int32_t tiles_log2, pad2;
   int64_t batch;
   const uint8_t* paulis;
+  const R* tmats;  // per-trajectory matrices of SK_TMAT records (point * batch + state)
   int32_t pool_len;                      // matrix reals of this sweep (staged in shared memory)
   int32_t n_local_slots;                 // Pauli slots in this sweep
   int32_t slot_map[kSweepMaxGates + 1];  // local slot -> slot index of the choice table

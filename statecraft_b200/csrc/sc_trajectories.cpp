@@ -71,12 +71,15 @@ int weighted_index(const double* w, int count, double value) {
 
 constexpr double kMinKrausWeight = 1e-15;
 
-// One piece of the batch between two Kraus points: the fused plan of its gates and
-// Pauli slots, then (kraus >= 0) the noise record whose branch weights depend on the
-// state, drawn on the device.
+// One piece of the batch between two Kraus points: the fused plan of its gates, Pauli
+// slots and the matrix records of earlier Kraus points, then (kraus >= 0) the noise
+// record whose branch weights depend on the state, weighed and drawn on the device
+// (Kraus point number kp; with pend_kp >= 0, the matrix of that earlier point on
+// qubit pend_q is not applied yet and is applied while weighing).
 struct Segment {
   Plan plan;
-  int64_t kraus = -1;
+  int64_t kraus = -1, kp = -1, pend_kp = -1;
+  int pend_q = -1;
 };
 
 // Offsets in the trajectory scratch buffer
@@ -85,7 +88,7 @@ struct AuxLayout {
 };
 
 AuxLayout aux_layout(size_t n_codes, uint64_t chunks, int64_t n_traj, int64_t shots,
-                     int64_t n_kraus_pts, int kraus_gx) {
+                     int64_t n_kraus_pts, int kraus_gx, size_t real_bytes) {
   auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
   const size_t T = (size_t)n_traj;
   AuxLayout a;
@@ -99,7 +102,7 @@ AuxLayout aux_layout(size_t n_codes, uint64_t chunks, int64_t n_traj, int64_t sh
   a.out = up(a.scalars + sizeof(SampleScalars) * T);
   a.partial = up(a.out + sizeof(int32_t) * (size_t)std::max<int64_t>(1, shots * n_traj));
   a.mats = up(a.partial + sizeof(double) * SC_MAX_KRAUS * (size_t)kraus_gx * T);
-  a.kchoice = up(a.mats + 8 * sizeof(double) * T);
+  a.kchoice = up(a.mats + 8 * real_bytes * T * (size_t)std::max<int64_t>(1, n_kraus_pts));
   a.status = up(a.kchoice + sizeof(int32_t) * T * (size_t)std::max<int64_t>(1, n_kraus_pts));
   a.bytes = up(a.status + sizeof(int32_t) * T);
   return a;
@@ -206,17 +209,40 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
     tc->key = key;
   }
 
-  // one gate list per segment: ops with a Pauli slot after each Pauli record; a
-  // Kraus point ends the segment
+  // One gate list per segment: ops with a Pauli slot after each Pauli record.  A
+  // Kraus point ends the segment; its drawn matrix is applied by a matrix record at
+  // the head of the next gate list.  Back-to-back Kraus points on two qubits (the
+  // records after a two-qubit gate) share one segment boundary: the second is weighed
+  // with the first's matrix applied on the fly.
   auto build_segments = [&](const PlanParams& pp, std::vector<Segment>* out) -> int {
     out->clear();
     std::vector<PGate> gates;
-    int64_t next = 0;
-    auto close_segment = [&](int64_t kraus) -> int {
+    std::vector<std::pair<int64_t, int>> pending;  // (Kraus point, qubit) not in a list yet
+    int64_t next = 0, kp_count = 0;
+    auto flush_pending = [&](int64_t op) {
+      for (const auto& pe : pending) {
+        PGate tm;
+        std::memset(&tm, 0, sizeof tm);
+        tm.kind = PK_TMAT;
+        tm.q0 = pe.second;
+        tm.q1 = (int32_t)pe.first;
+        tm.op_index = op;
+        gates.push_back(tm);
+      }
+      pending.clear();
+    };
+    auto close_segment = [&](int64_t kraus, int64_t kp) -> int {
       Segment sg;
-      sg.plan = plan_sweeps(gates, n, pp);
-      if (!sg.plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+      if (!gates.empty()) {
+        sg.plan = plan_sweeps(gates, n, pp);
+        if (!sg.plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+      }
       sg.kraus = kraus;
+      sg.kp = kp;
+      if (kraus >= 0 && !pending.empty()) {
+        sg.pend_kp = pending[0].first;
+        sg.pend_q = pending[0].second;
+      }
       out->push_back(std::move(sg));
       gates.clear();
       return SC_OK;
@@ -227,11 +253,13 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
       if (!normalise_op(ops[i], nullptr, 0, &g, &produced))
         return fail(SC_EINVAL, "op %lld: cannot normalise", (long long)i);
       if (produced) {
+        flush_pending(i);
         g.op_index = i;
         gates.push_back(g);
       }
       while (next < n_channels && ch[next].after_op == i) {
         if (is_pauli[next]) {
+          flush_pending(i);
           PGate sl;
           std::memset(&sl, 0, sizeof sl);
           sl.kind = PK_PAULI;
@@ -240,13 +268,19 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
           sl.op_index = i;
           gates.push_back(sl);
         } else {
-          const int r = close_segment(next);
+          const int q = ch[next].target;
+          if (pending.size() > 1 || (pending.size() == 1 && pending[0].second == q))
+            flush_pending(i);
+          const int r = close_segment(next, kp_count);
           if (r != SC_OK) return r;
+          pending.emplace_back(kp_count++, q);
         }
         ++next;
       }
     }
-    return close_segment(-1);
+    flush_pending(n_ops - 1);
+    if (!gates.empty()) return close_segment(-1, -1);
+    return SC_OK;
   };
   auto shape_params = [&](int tile, int nr) {
     PlanParams pp = c->plan_params();
@@ -278,7 +312,7 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
   const size_t state_bytes = amp * len * (size_t)n_traj;
   const uint64_t chunks = sample_chunks(len);
   const int kraus_gx = noise_grid_batch(n, n_traj, c->sm_count);
-  const AuxLayout L = aux_layout(paulis.size(), chunks, n_traj, shots, n_kp, kraus_gx);
+  const AuxLayout L = aux_layout(paulis.size(), chunks, n_traj, shots, n_kp, kraus_gx, amp / 2);
   if ((rc = c->reserve(c->buf_traj_states, state_bytes, "trajectory states")) != SC_OK) return rc;
   if ((rc = c->reserve(c->buf_traj_aux, L.bytes, "trajectory scratch")) != SC_OK) return rc;
   if ((rc = c->reserve(c->buf_err, 16, "error flag")) != SC_OK) return rc;
@@ -317,13 +351,12 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
     r = launch_init_batch(c->cfg.dtype, c->buf_traj_states.p, n, n_traj, s);
     c->mark_end();
     if (r != cudaSuccess) return r;
-    int64_t kp = 0;
     for (const Segment& sg : segs) {
       for (size_t k = 0; k < sg.plan.sweeps.size(); ++k) {
         c->mark_begin(KC_SWEEP, 2.0 * dim * (double)amp * (double)n_traj);
         r = launch_sweep_batch(c->cfg.dtype, c->buf_traj_states.p, n, n_traj, sg.plan, k,
                                reinterpret_cast<const uint8_t*>(aux + L.codes), (int)n_ch,
-                               static_cast<int*>(c->buf_err.p), c->sm_count, s);
+                               aux + L.mats, static_cast<int*>(c->buf_err.p), c->sm_count, s);
         c->mark_end();
         if (r != cudaSuccess) return r;
       }
@@ -334,15 +367,17 @@ int32_t sc_trajectories(void* p, int32_t n, const sc_op* ops, int64_t n_ops,
       ka.nk = rec.n_kraus;
       ka.target = rec.target;
       for (int k = 0; k < rec.n_kraus; ++k) std::memcpy(ka.k[k], rec.kraus[k], 8 * sizeof(double));
-      c->mark_begin(KC_NOISE, 3.0 * dim * (double)amp * (double)n_traj, 3);
-      r = launch_kraus_batch(c->cfg.dtype, c->buf_traj_states.p, n, n_traj, ka, seeds_dev,
-                             (uint64_t)sg.kraus, reinterpret_cast<double*>(aux + L.partial),
-                             reinterpret_cast<double*>(aux + L.mats),
-                             reinterpret_cast<int32_t*>(aux + L.kchoice) + kp, n_kp, status_dev,
+      const size_t mat_bytes = 4 * amp * (size_t)n_traj;  // one Kraus point's matrices
+      c->mark_begin(KC_NOISE, dim * (double)amp * (double)n_traj, 2);
+      r = launch_kraus_batch(c->cfg.dtype, c->buf_traj_states.p, n, n_traj, ka, sg.pend_q,
+                             sg.pend_kp >= 0 ? aux + L.mats + sg.pend_kp * mat_bytes : nullptr,
+                             seeds_dev, (uint64_t)sg.kraus,
+                             reinterpret_cast<double*>(aux + L.partial),
+                             aux + L.mats + sg.kp * mat_bytes,
+                             reinterpret_cast<int32_t*>(aux + L.kchoice) + sg.kp, n_kp, status_dev,
                              c->sm_count, s);
       c->mark_end();
       if (r != cudaSuccess) return r;
-      ++kp;
     }
     if (sample && shots > 0) {
       c->mark_begin(KC_SAMPLE, dim * (double)amp * (double)n_traj, kSampleKernels);

@@ -138,7 +138,8 @@ def test_histograms_match_oracle(ctx):
 
 
 def _channel_records(circuit, channels):
-    """channels[k % len] after gate k, on every qubit the gate touches"""
+    """channels[k % len] after gate k, on every qubit the gate touches (a tuple entry:
+    each of its channels in turn on each qubit)"""
     out = []
     from statecraft_b200 import quantum as Q
     for i, op in enumerate(circuit.operations):
@@ -147,10 +148,11 @@ def _channel_records(circuit, channels):
         chan = channels[i % len(channels)]
         if chan is None:
             continue
-        kraus = tuple(np.array(k.matrix, dtype=complex).reshape(2, 2)
-                      for k in chan.krausDecomposition())
         for q in sorted(op.qubits_touched()):
-            out.append(N.FlatChannel(i, q, kraus))
+            for ch in (chan if isinstance(chan, tuple) else (chan,)):
+                kraus = tuple(np.array(k.matrix, dtype=complex).reshape(2, 2)
+                              for k in ch.krausDecomposition())
+                out.append(N.FlatChannel(i, q, kraus))
     return out
 
 
@@ -160,6 +162,9 @@ _CHANNELS = {
     "thermal": [N.ThermalRelaxationChannel(50.0, 70.0, 9.0, (0,))],
     "mixed": [N.AmplitudeDampingChannel(0.15, (0,)), N.DepolarizingChannel(0.2, (0,)), None,
               N.PhaseDampingChannel(0.25, (0,)), N.PhaseFlipChannel(0.3, (0,))],
+    # two state-dependent records on the same qubit back to back
+    "stacked": [(N.AmplitudeDampingChannel(0.2, (0,)), N.PhaseDampingChannel(0.2, (0,))),
+                (N.DepolarizingChannel(0.1, (0,)), N.AmplitudeDampingChannel(0.25, (0,)))],
 }
 
 
@@ -170,6 +175,8 @@ def test_state_dependent_channels_match_oracle(ctx, kind):
     n, traj = 9, 12
     c = RCirc.random_circuit(n, 40, seed=910)
     rec = _channel_records(c, _CHANNELS[kind])
+    # records after gates on three or more qubits (multi-controlled gates) included
+    assert max(len(op.qubits_touched()) for op in c.operations) >= 3
     res = run_trajectories(c, rec, traj, noise_seed=313, shots=0, measure_seed=0,
                            return_states=True, context=ctx)
     for t in range(traj):
