@@ -321,79 +321,88 @@ __device__ double warp_exact_starts(const Get& get, uint32_t n, double S, int la
 
 // pass C: per chunk, the binade its running sum stays in (from the approximate
 // running sums, with a margin of 2^-18 relative, far above the summation error of at
-// most 2^32 * 2^-53 relative) and its effect there
+// most 2^32 * 2^-53 relative) and its effect there.  One warp per chunk, in four
+// sub-blocks of 512 values: a coalesced load into the warp's shared slab (padded one
+// double per 16), then lane l takes the sub-block's values [16 l, 16 l + 16)
+// (contiguous, so the lanes' effects compose in lane order), a warp scan, and the
+// sub-block effects composed in order.  A chunk with no binade is checked for being
+// all zeros.
+constexpr int kSubBlock = 512;
+constexpr int kSlab = kSubBlock + kSubBlock / 16;
+
 template <typename Src>
 __global__ void __launch_bounds__(kThreadsA) k_chunk_tf(Src src, uint64_t len_per,
                                                         uint64_t chunks_per, uint64_t chunks,
                                                         const double* prefix,
                                                         const SampleScalars* sc,
                                                         bool scaled_pass, ChunkTf* out) {
-  __shared__ Tf wtf[kThreadsA / 32];
-  __shared__ int s_e, s_bad;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   constexpr double kMargin = 0x1p-18;
-  for (uint64_t c = blockIdx.x; c < chunks; c += gridDim.x) {
+  constexpr int seg = kSubBlock / 32;
+  __shared__ double slab_all[kThreadsA / 32][kSlab];
+  const int lane = threadIdx.x & 31;
+  double* const slab = slab_all[threadIdx.x >> 5];
+  const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  for (uint64_t c = warp0; c < chunks; c += nwarps) {
     const uint64_t st = c / chunks_per;
     if (scaled_pass && !sc[st].scaled) continue;
     const double scale = scaled_pass ? sc[st].scale : 1.0;
     const uint64_t cl = c - st * chunks_per;
-    if (threadIdx.x == 0) {
-      // clean: the whole chunk inside [2^e, 2^(e+1)) with the margin on both ends (the
-      // last chunk, whose end is the total, is always added element by element)
-      bool clean = cl + 1 < chunks_per;
-      int e = -2000;
-      if (clean) {
-        // on the rescaled pass the running sums of the unscaled probabilities times the
-        // scale stand in for those of the scaled ones (relative error ~2^-52 per value)
-        const double a = prefix[c] * scale, b = prefix[c + 1] * scale;
-        e = binade(a * (1.0 - kMargin));
-        clean = e > -1000 && binade(a) == e && binade(b * (1.0 + kMargin)) == e;
-      }
-      s_e = clean ? e : -2000;
-      s_bad = 0;
+    // clean: the whole chunk inside [2^e, 2^(e+1)) with the margin on both ends (the
+    // last chunk, whose end is the total, is always added element by element).  On
+    // the rescaled pass the running sums of the unscaled probabilities times the scale
+    // stand in for those of the scaled ones (relative error ~2^-52 per value).
+    int e = -2000;
+    if (cl + 1 < chunks_per) {
+      const double a = prefix[c] * scale, b = prefix[c + 1] * scale;
+      const int ea = binade(a * (1.0 - kMargin));
+      if (ea > -1000 && binade(a) == ea && binade(b * (1.0 + kMargin)) == ea) e = ea;
     }
-    __syncthreads();
-    const int e = s_e;
-    const uint64_t b0 = cl * kChunk + (uint64_t)threadIdx.x * (kChunk / kThreadsA);
     const uint64_t off = st * len_per;
-    if (e < -1000) {
-      // a chunk of zeros is the identity whatever the running sum (a sum of values
-      // >= 0 is zero only when every value is)
-      bool nz = false;
-      for (int k = 0; k < kChunk / kThreadsA; ++k) {
-        const uint64_t i = b0 + k;
-        if (i >= len_per) break;
-        double pv = src(off + i);
+    const uint64_t b0 = cl * kChunk;
+    bool nz = false, bad = false;
+    Tf total = tf_identity();
+    for (int sb = 0; sb < kChunk / kSubBlock; ++sb) {
+      const uint64_t base = b0 + (uint64_t)sb * kSubBlock;
+      __syncwarp();  // the previous sub-block's reads of the slab are done
+#pragma unroll
+      for (int k = 0; k < seg; ++k) {
+        const int q = k * 32 + lane;
+        const uint64_t i = base + q;
+        double pv = i < len_per ? src(off + i) : 0.0;
         if (scaled_pass) pv = __dmul_rn(pv, scale);
-        nz = nz || pv != 0.0;
+        slab[q + (q >> 4)] = pv;
       }
-      const bool any_nz = __syncthreads_or(nz);
-      if (threadIdx.x == 0) out[c] = ChunkTf{0, 0, any_nz ? 0 : (2 | kTfZero), -2000};
-      __syncthreads();
+      __syncwarp();
+      if (e < -1000) {
+        // a chunk of zeros is the identity whatever the running sum (a sum of
+        // values >= 0 is zero only when every value is)
+#pragma unroll
+        for (int k = 0; k < seg; ++k) nz = nz || slab[k * 32 + lane + ((k * 32 + lane) >> 4)] != 0.0;
+        continue;
+      }
+      Tf t = tf_identity();
+      const int q0 = lane * seg;
+#pragma unroll
+      for (int k = 0; k < seg; ++k) {
+        const int q = q0 + k;
+        t = tf_compose(t, tf_of(slab[q + (q >> 4)], e, &bad));
+      }
+      t = tf_warp_scan(t, lane);
+      Tf sbt;  // the sub-block's effect, from lane 31
+      sbt.d0 = __shfl_sync(0xffffffffu, t.d0, 31);
+      sbt.d1 = __shfl_sync(0xffffffffu, t.d1, 31);
+      sbt.p = __shfl_sync(0xffffffffu, t.p, 31);
+      total = tf_compose(total, sbt);
+    }
+    if (e < -1000) {
+      const bool any_nz = __any_sync(0xffffffffu, nz);
+      if (lane == 0) out[c] = ChunkTf{0, 0, any_nz ? 0 : (2 | kTfZero), -2000};
       continue;
     }
-    bool bad = false;
-    Tf t = tf_identity();
-    for (int k = 0; k < kChunk / kThreadsA; ++k) {
-      const uint64_t i = b0 + k;
-      if (i >= len_per) break;
-      double pv = src(off + i);
-      if (scaled_pass) pv = __dmul_rn(pv, scale);
-      t = tf_compose(t, tf_of(pv, e, &bad));
-    }
-    t = tf_warp_scan(t, lane);
     const bool any_bad = __any_sync(0xffffffffu, bad);
-    if (lane == 31) {
-      wtf[warp] = t;
-      if (any_bad) s_bad = 1;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      Tf r = tf_identity();
-      for (int w = 0; w < kThreadsA / 32; ++w) r = tf_compose(r, wtf[w]);
-      out[c] = ChunkTf{r.d0, r.d1, (int32_t)(r.p & 3u) | (s_bad ? 0 : kTfUsable), e};
-    }
-    __syncthreads();
+    if (lane == 0)
+      out[c] = ChunkTf{total.d0, total.d1, (int32_t)(total.p & 3u) | (any_bad ? 0 : kTfUsable), e};
   }
 }
 
@@ -699,6 +708,7 @@ cudaError_t sample_src(Src src, uint64_t len, int64_t batch, const SampleArgs& a
   const uint64_t chunks = (len + kChunk - 1) / kChunk;
   const uint64_t all_chunks = chunks * (uint64_t)batch;
   const int grid_chunks = grid_cap(all_chunks * kThreadsA, kThreadsA, a.sm_count);
+  const int grid_warps = grid_cap(all_chunks * 32, kThreadsA, a.sm_count);
   cudaError_t e = cudaMemsetAsync(a.scalars, 0, sizeof(SampleScalars) * (size_t)batch, s);
   if (e != cudaSuccess) return e;
   // the running sum of the probabilities, then (decided on the device, per state) of
@@ -709,7 +719,7 @@ cudaError_t sample_src(Src src, uint64_t len, int64_t batch, const SampleArgs& a
                                                           all_chunks);
       k_prefix_approx<<<(unsigned)batch, 1024, 0, s>>>(a.chunk_sums, chunks, a.chunk_prefix);
     }
-    k_chunk_tf<Src><<<grid_chunks, kThreadsA, 0, s>>>(src, len, chunks, all_chunks,
+    k_chunk_tf<Src><<<grid_warps, kThreadsA, 0, s>>>(src, len, chunks, all_chunks,
                                                       a.chunk_prefix, a.scalars, pass == 1,
                                                       a.chunk_tf);
     k_exact_starts<Src><<<(unsigned)batch, 1024, 0, s>>>(src, len, chunks, a.chunk_tf,
