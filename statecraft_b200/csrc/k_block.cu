@@ -10,7 +10,10 @@
 // parts) is staged once per CTA in shared memory; each warp stages its 8 columns in a
 // shared slab (coalesced: for one row, the 8 columns are consecutive when the lowest
 // qubit is not in the block), keeps its B fragments in registers, and writes Y back
-// through the same slab.  complex128 only (complex64 states keep the sweep path).
+// through the same slab.  Slab rows are padded to 9 entries (the fragment stores of
+// 8 rows x 4 lanes hit distinct 16-byte bank groups) and U's rows to D + 4 doubles
+// (the A fragments' 4 rows x 4 columns per half-warp hit distinct banks).
+// complex128 only (complex64 states keep the sweep path).
 #include <algorithm>
 
 #include "sc_device.cuh"
@@ -21,6 +24,7 @@ namespace sc {
 namespace {
 
 constexpr int kBlockWarps = 8;
+constexpr int kSlabRow = 9;  // slab row stride in entries (8 columns + 1 pad)
 
 // D = 2^k rows and columns of U; BlockArgs carries the block's qubits (ascending)
 template <int D>
@@ -30,13 +34,15 @@ __global__ void __launch_bounds__(kBlockWarps * 32)
   constexpr int MT = D / 8;   // row tiles
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double* const ur = reinterpret_cast<double*>(smem_raw);  // [D][D]
-  double* const ui = ur + D * D;
-  double2* const slabs = reinterpret_cast<double2*>(ui + D * D);
+  constexpr int UR = D + 4;  // U row stride in doubles
+  double* const ui = ur + D * UR;
+  double2* const slabs = reinterpret_cast<double2*>(ui + D * UR);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double2* const xs = slabs + warp * (D * 8);  // [row][col]
+  double2* const xs = slabs + warp * (D * kSlabRow);  // [row][col]
   for (int e = threadIdx.x; e < D * D; e += blockDim.x) {
-    ur[e] = u[2 * e];
-    ui[e] = u[2 * e + 1];
+    const int at = (e / D) * UR + e % D;
+    ur[at] = u[2 * e];
+    ui[at] = u[2 * e + 1];
   }
   __syncthreads();
   const int k = a.k;
@@ -61,13 +67,13 @@ __global__ void __launch_bounds__(kBlockWarps * 32)
        gidx += (uint64_t)gridDim.x * kBlockWarps) {
     const uint64_t base = col_base(gidx * 8 + ln);
 #pragma unroll
-    for (int j = lr; j < D; j += 4) xs[j * 8 + ln] = st[base | row_off(j)];
+    for (int j = lr; j < D; j += 4) xs[j * kSlabRow + ln] = st[base | row_off(j)];
     __syncwarp();
     // B fragments (4 x 8, column-major): lane holds row kt*4 + lane%4, column lane/4
     double br[KT], bi[KT];
 #pragma unroll
     for (int kt = 0; kt < KT; ++kt) {
-      const double2 x = xs[(kt * 4 + (lane & 3)) * 8 + (lane >> 2)];
+      const double2 x = xs[(kt * 4 + (lane & 3)) * kSlabRow + (lane >> 2)];
       br[kt] = x.x;
       bi[kt] = x.y;
     }
@@ -78,7 +84,7 @@ __global__ void __launch_bounds__(kBlockWarps * 32)
 #pragma unroll
       for (int kt = 0; kt < KT; ++kt) {
         // A fragment (8 x 4, row-major): lane holds row lane/4, column lane%4
-        const int ao = (mt * 8 + (lane >> 2)) * D + kt * 4 + (lane & 3);
+        const int ao = (mt * 8 + (lane >> 2)) * UR + kt * 4 + (lane & 3);
         const double ar = ur[ao], ai = ui[ao];
         asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
                      : "+d"(yr0), "+d"(yr1) : "d"(ar), "d"(br[kt]));
@@ -91,12 +97,12 @@ __global__ void __launch_bounds__(kBlockWarps * 32)
       }
       // C fragment (8 x 8): lane holds row lane/4, columns 2 (lane%4) and 2 (lane%4) + 1
       const int row = mt * 8 + (lane >> 2), c0 = 2 * (lane & 3);
-      xs[row * 8 + c0] = make_double2(yr0 - zr0, yi0);
-      xs[row * 8 + c0 + 1] = make_double2(yr1 - zr1, yi1);
+      xs[row * kSlabRow + c0] = make_double2(yr0 - zr0, yi0);
+      xs[row * kSlabRow + c0 + 1] = make_double2(yr1 - zr1, yi1);
     }
     __syncwarp();
 #pragma unroll
-    for (int j = lr; j < D; j += 4) st[base | row_off(j)] = xs[j * 8 + ln];
+    for (int j = lr; j < D; j += 4) st[base | row_off(j)] = xs[j * kSlabRow + ln];
     __syncwarp();
   }
 }
@@ -104,7 +110,8 @@ __global__ void __launch_bounds__(kBlockWarps * 32)
 template <int D>
 cudaError_t launch_d(double2* st, int n, const BlockArgs& a, const double* u, int sm_count,
                      cudaStream_t s) {
-  const size_t smem = 2 * sizeof(double) * D * D + sizeof(double2) * D * 8 * kBlockWarps;
+  const size_t smem =
+      2 * sizeof(double) * D * (D + 4) + sizeof(double2) * D * kSlabRow * kBlockWarps;
   auto kern = k_block<D>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;

@@ -969,8 +969,11 @@ __device__ __forceinline__ double probe_sum(const typename Amp<R>::type (&v)[1 <
   return s;
 }
 
-template <typename R, int NR>
-__global__ void __launch_bounds__(256, 2)
+// THREADS threads per tile, MINB CTAs per SM (their register cap: 65536 / (THREADS x
+// MINB)).  While a tile computes, each thread asks L2 for its amplitudes of the
+// CTA's next tile (`prefetch.global.L2`: no registers, no wait).
+template <typename R, int NR, int THREADS, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB)
     k_adjoint_sweep(typename Amp<R>::type* __restrict__ psi, typename Amp<R>::type* __restrict__ lam,
                     const __grid_constant__ SweepParams<R> p, double* __restrict__ partial,
                     int n_probes) {
@@ -998,6 +1001,14 @@ __global__ void __launch_bounds__(256, 2)
     for (int j = 0; j < NV; ++j) {
       v[j] = psi[base | gt_first | p.gfirst[j]];
       w[j] = lam[base | gt_first | p.gfirst[j]];
+    }
+    if (t + gridDim.x < (uint32_t)p.tiles) {
+      const uint32_t nb = tile_base(t + gridDim.x, p);
+#pragma unroll
+      for (int j = 0; j < NV; ++j) {
+        prefetch_l2(psi + (nb | gt_first | p.gfirst[j]));
+        prefetch_l2(lam + (nb | gt_first | p.gfirst[j]));
+      }
     }
     uint32_t l0 = l0_first, psw0 = 0;
     RegOff<NR> off;
@@ -1736,8 +1747,10 @@ cudaError_t launch_adjoint_t(void* psi, void* lam, const Plan& plan, size_t k, d
   }
   const int threads = 1 << (p.T - p.nr);
   if (threads < 32 || threads > 256) return cudaErrorInvalidValue;
+  // 256-thread tiles at two CTAs per SM (128 registers); smaller tiles at three
+  // (170 registers: the two states' registers without spills)
   const size_t smem = 2 * (sizeof(A) << p.T) + sizeof(double) * (size_t)n_probes * (threads / 32);
-  auto kern = k_adjoint_sweep<R, 3>;
+  auto kern = threads == 256 ? k_adjoint_sweep<R, 3, 256, 2> : k_adjoint_sweep<R, 3, 128, 3>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;

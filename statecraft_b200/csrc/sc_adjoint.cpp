@@ -6,6 +6,7 @@
 // and gradient probes; otherwise gate by gate, three passes per rotation.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -112,12 +113,17 @@ int reserve_scratch(Ctx* c, int64_t n_params) {
                     "adjoint scratch");
 }
 
-// Sweep shape of the reverse pass: 2048-amplitude tiles, 3 register qubits (both
-// states' registers in one thread), plain matrix records.
+// Sweep shape of the reverse pass: 3 register qubits (both states' registers in one
+// thread), plain matrix records; 2048-amplitude tiles (256 threads) unless
+// STATECRAFT_B200_ADJOINT_TILE sets the tile qubits (10: 128-thread tiles).
 PlanParams reverse_plan_params(const Ctx* c) {
   PlanParams pp;
   const bool c64 = c->cfg.dtype == SC_C64;
   pp.tile_qubits = 11;
+  if (const char* v = getenv("STATECRAFT_B200_ADJOINT_TILE")) {
+    const int t = atoi(v);
+    if (t >= 8 && t <= 11) pp.tile_qubits = t;
+  }
   pp.low_qubits = c64 ? 5 : 4;
   pp.nr = 3;
   pp.budget = -1.0;
