@@ -242,7 +242,8 @@ SC_API int32_t sc_last_plan_stats(void* ctx, int64_t* sweeps, int64_t* gates, in
  * own buffers.  Samples every qubit of a state the caller holds in device memory
  * (d_state: 2^n amplitudes of `dtype`; outcome = basis index) into the caller's
  * device buffer d_outcomes[shots], on the caller's cudaStream_t `stream`, and
- * returns after the stream has finished.
+ * returns after the stream has finished (on a stream that is capturing it returns
+ * SC_EINVAL and enqueues nothing).
  * Uniforms: d_uniforms[shot] (device, nullable) else SplittableRandom(seed).
  * Scratch is a fixed array in the library's device data sized for at most 2^30
  * amplitudes (30 qubits, about 24 MiB held by every GPU that loads the library);

@@ -330,11 +330,12 @@ __device__ __forceinline__ void d1r(typename Amp<R>::type (&v)[1 << NR], const R
 // Rotation form of commuting 2x2 gates on the register bits of mask M: each gate is
 // diag(1, e^{i phi}) [[1, -t], [t, 1]] diag(1, e^{i lam}) (its scalar is applied by
 // the sweep), and since the gates act on distinct bits their input and output
-// phases combine into one diagonal each.  Pool: t per bit (ascending), then the
-// input-phase table lam[s] and the output-phase table phi[s], complex, for
+// phases combine into one diagonal each.  Pool: t per bit (ascending), t / (1 + t^2)
+// per bit, then the input-phase table lam[s] (which also carries the real factors
+// 1 + t^2 of the bits in s) and the output-phase table phi[s], complex, for
 // s = 1 .. 2^K - 1 (s = the bits of j in M, compacted; s = 0 is the phase 1).
 // A 4-bit record costs 15 + 15 complex multiplies and 4 x 8 rotations (248 FP64
-// operations for 16 amplitudes) where four single-bit gates cost 384.
+// operations for 16 amplitudes, all in place) where four single-bit gates cost 384.
 template <int M>
 __host__ __device__ constexpr int compact_bits(int j) {
   int s = 0, k = 0;
@@ -343,15 +344,20 @@ __host__ __device__ constexpr int compact_bits(int j) {
   return s;
 }
 
+// [[1, -t], [t, 1]] on register bit A_ as two shears, the amplitude on the 1 side
+// arriving scaled by 1 + t^2 (the record's input table): a0 -= tp a1, a1 += t a0 with
+// tp = t / (1 + t^2).  Each update overwrites the value it reads last, so the pair
+// stays in its registers (no temporaries to move back at the record's end).
 template <typename R, int NR, int A_>
-__device__ __forceinline__ void rot(typename Amp<R>::type (&v)[1 << NR], const R t) {
+__device__ __forceinline__ void rot(typename Amp<R>::type (&v)[1 << NR], const R t, const R tp) {
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j) {
     if (j & (1 << A_)) continue;
     const int j1 = j | (1 << A_);
-    const auto a0 = v[j], a1 = v[j1];
-    v[j] = make_amp<R>(fma(-t, a1.x, a0.x), fma(-t, a1.y, a0.y));
-    v[j1] = make_amp<R>(fma(t, a0.x, a1.x), fma(t, a0.y, a1.y));
+    v[j].x = fma(-tp, v[j1].x, v[j].x);
+    v[j].y = fma(-tp, v[j1].y, v[j].y);
+    v[j1].x = fma(t, v[j].x, v[j1].x);
+    v[j1].y = fma(t, v[j].y, v[j1].y);
   }
 }
 
@@ -367,14 +373,14 @@ __device__ __forceinline__ void phase_table(typename Amp<R>::type (&v)[1 << NR],
 template <typename R, int NR, int M>
 __device__ __forceinline__ void g1allq(typename Amp<R>::type (&v)[1 << NR], const R* q) {
   constexpr int K = ((M >> 0) & 1) + ((M >> 1) & 1) + ((M >> 2) & 1) + ((M >> 3) & 1);
-  const R* lam = q + K;
+  const R* lam = q + 2 * K;
   const R* phi = lam + 2 * ((1 << K) - 1);
   phase_table<R, NR, M>(v, lam);
   const R* tq = q;
-  if constexpr ((M & 1) != 0) rot<R, NR, 0>(v, *tq++);
-  if constexpr (NR > 1 && (M & 2) != 0) rot<R, NR, 1>(v, *tq++);
-  if constexpr (NR > 2 && (M & 4) != 0) rot<R, NR, 2>(v, *tq++);
-  if constexpr (NR > 3 && (M & 8) != 0) rot<R, NR, 3>(v, *tq);
+  if constexpr ((M & 1) != 0) { rot<R, NR, 0>(v, tq[0], tq[K]); ++tq; }
+  if constexpr (NR > 1 && (M & 2) != 0) { rot<R, NR, 1>(v, tq[0], tq[K]); ++tq; }
+  if constexpr (NR > 2 && (M & 4) != 0) { rot<R, NR, 2>(v, tq[0], tq[K]); ++tq; }
+  if constexpr (NR > 3 && (M & 8) != 0) rot<R, NR, 3>(v, tq[0], tq[K]);
   phase_table<R, NR, M>(v, phi);
 }
 
@@ -464,6 +470,38 @@ __device__ __forceinline__ void prex(typename Amp<R>::type (&v)[1 << NR], uint32
   if constexpr (NR > 3) {
     if (b & 8u) xswap0<R, NR, 3>(v);
   }
+}
+
+// real rotations on the register bits of mask M as lifting shears (pool: p, s per
+// bit, ascending): a0 += p a1, a1 += s a0, a0 += p a1, every update in place
+template <typename R, int NR, int M>
+__device__ __forceinline__ void rotl(typename Amp<R>::type (&v)[1 << NR], const R* q) {
+#pragma unroll
+  for (int b = 0, k = 0; b < NR; ++b) {
+    if (!((M >> b) & 1)) continue;
+    const R pp = q[2 * k], ss = q[2 * k + 1];
+    ++k;
+#pragma unroll
+    for (int j = 0; j < (1 << NR); ++j) {
+      if (j & (1 << b)) continue;
+      const int j1 = j | (1 << b);
+      v[j].x = fma(pp, v[j1].x, v[j].x);
+      v[j].y = fma(pp, v[j1].y, v[j].y);
+      v[j1].x = fma(ss, v[j].x, v[j1].x);
+      v[j1].y = fma(ss, v[j].y, v[j1].y);
+      v[j].x = fma(pp, v[j1].x, v[j].x);
+      v[j].y = fma(pp, v[j1].y, v[j].y);
+    }
+  }
+}
+
+// diag(1, d) on register bit A_: only the registers with the bit set change
+template <typename R, int NR, int A_>
+__device__ __forceinline__ void d1h(typename Amp<R>::type (&v)[1 << NR], const R* m) {
+  const R dr = m[0], di = m[1];
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j)
+    if ((j >> A_) & 1) v[j] = cmul(dr, di, v[j]);
 }
 
 // diagonal over the register bits as a table: register j times entry j
@@ -896,6 +934,9 @@ __device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 <
       rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(w)
 #define SC_DO_X0(A) xswap0<R, NR, A>(v), xswap0<R, NR, A>(w)
 #define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v), cxswap0<R, NR, A, B>(w)
+#define SC_DO_D1H(A) d1h<R, NR, A>(v, m), d1h<R, NR, A>(w, m)
+    SC_CASES_1(SK_D1H, SC_DO_D1H)
+#undef SC_DO_D1H
     SC_CASES_1(SK_G1, SC_DO_G1)
     SC_CASES_1(SK_X, SC_DO_X)
     SC_CASES_1(SK_D1R, SC_DO_D1R)
@@ -924,6 +965,16 @@ __device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 <
     SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
     SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
 #undef SC_G1ALL_CASE
+#define SC_ROTL_CASE(M)                         \
+  case (SK_ROTL << 4) | (M):                    \
+    if constexpr (((M) >> NR) == 0) {           \
+      rotl<R, NR, (M)>(v, m);                   \
+      rotl<R, NR, (M)>(w, m);                   \
+    }                                           \
+    break;
+    SC_ROTL_CASE(1) SC_ROTL_CASE(2) SC_ROTL_CASE(3) SC_ROTL_CASE(4)
+    SC_ROTL_CASE(5) SC_ROTL_CASE(6) SC_ROTL_CASE(7)
+#undef SC_ROTL_CASE
     case SK_DTAB << 4:
       dtab<R, NR>(v, m);
       dtab<R, NR>(w, m);
@@ -1718,7 +1769,10 @@ bool adjoint_plan_supported(const Plan& plan) {
       switch (plan.gates[g].kind) {
         case SK_G1: case SK_X: case SK_SWAP: case SK_D1: case SK_D2: case SK_DP:
         case SK_CX: case SK_DPR: case SK_G1ALL: case SK_D1R: case SK_X0: case SK_CX0: case SK_DTAB:
-        case SK_PROBE:
+        case SK_PROBE: case SK_D1H:
+          break;
+        case SK_ROTL:  // NR = 3: masks of three register bits
+          if (plan.gates[g].a & ~7) return false;
           break;
         default: return false;
       }

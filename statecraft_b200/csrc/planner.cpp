@@ -249,6 +249,29 @@ bool rotation_form(const double* u, double min_c, double* q, double* fr, double*
   return true;
 }
 
+// A 2x2 unitary u that is e^{ig} [[cos al, -sin al], [sin al, cos al]] (a real
+// rotation up to a phase): the lifting shears of al reduced to |al| <= pi/2 (the
+// reduction by pi is a sign, itself a phase): q = {-tan(al/2), sin al}.
+bool lifted_rotation(const double* u, double* q) {
+  constexpr double kTol = 1e-13;
+  if (std::hypot(u[0] - u[6], u[1] - u[7]) > kTol || std::hypot(u[2] + u[4], u[3] + u[5]) > kTol)
+    return false;
+  const double c0 = std::hypot(u[0], u[1]), s0 = std::hypot(u[4], u[5]);
+  if (std::fabs(c0 * c0 + s0 * s0 - 1.0) > kTol) return false;
+  // the common phase, from the larger of u00 and u10
+  const double gr = c0 >= s0 ? u[0] / c0 : u[4] / s0, gi = c0 >= s0 ? u[1] / c0 : u[5] / s0;
+  // u00 e^{-ig} and u10 e^{-ig} must be real
+  const double cr = u[0] * gr + u[1] * gi, ci = u[1] * gr - u[0] * gi;
+  const double sr = u[4] * gr + u[5] * gi, si = u[5] * gr - u[4] * gi;
+  if (std::fabs(ci) > kTol || std::fabs(si) > kTol) return false;
+  double al = std::atan2(sr, cr);
+  if (al > 0.5 * M_PI) al -= M_PI;
+  if (al < -0.5 * M_PI) al += M_PI;
+  q[0] = -std::tan(0.5 * al);
+  q[1] = std::sin(al);
+  return true;
+}
+
 // ---------------------------------------------------------------------------
 // Stage peephole: fewer records per stage.  Every record costs a dispatch and a
 // reconciliation of the register-resident amplitudes, so register-bit diagonals
@@ -271,12 +294,13 @@ uint32_t record_bits(const SwGate& g, const int* reg_of_pos) {
   };
   switch (g.kind) {
     case SK_G1: case SK_X: case SK_X0: case SK_D1R: case SK_PAULI: case SK_XF: case SK_TMAT:
+    case SK_D1H:
       f |= 1u << g.a;
       break;
     case SK_G2: case SK_CX: case SK_CX0: case SK_DPR: case SK_SWAP: case SK_CXF:
       f |= (1u << g.a) | (1u << g.b);
       break;
-    case SK_G1ALL: case SK_G1ALLQ: f |= (uint32_t)g.a & 15u; break;
+    case SK_G1ALL: case SK_G1ALLQ: case SK_ROTL: f |= (uint32_t)g.a & 15u; break;
     case SK_DTAB: f |= 15u; break;
     case SK_D1: reg(g.a); break;
     case SK_DP: case SK_D2: reg(g.a); reg(g.b); break;
@@ -372,7 +396,7 @@ bool merge_diagonal(const SwGate& g, const SwGate& d, bool after, std::vector<do
   }
   double d0r, d0i;
   diagonal_at(d, pool, 0, &d0r, &d0i);
-  const int base = g.moff + K + (after ? 2 * ((1 << K) - 1) : 0);
+  const int base = g.moff + 2 * K + (after ? 2 * ((1 << K) - 1) : 0);
   for (int s = 1; s < (1 << K); ++s) {
     int x = 0;
     for (int k = 0; k < K; ++k)
@@ -936,17 +960,27 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         sg.kind = SK_G1ALLQ;
         for (int i : part) sg.a |= 1 << run[i].first;
         for (int i : xpart) sg.b |= 1 << run[i].first;
-        // t per gate, then the input- and output-phase tables over the subsets s of
-        // the record's gates (bit k of s: gate k, in increasing register bit)
+        // t and t / (1 + t^2) per gate, then the input- and output-phase tables over
+        // the subsets s of the record's gates (bit k of s: gate k, in increasing
+        // register bit).  The input table also carries the real factor 1 + t_k^2 of
+        // every gate k in s: with the amplitude on the 1 side of bit k scaled by it,
+        // the rotation is two in-place shears, a0 -= t/(1+t^2) a1, a1 += t a0
+        // (= [[1, -t], [t, 1]] applied to the unscaled pair).
         const int K = (int)part.size();
         for (int k = 0; k < K; ++k) plan.pool.push_back(qs[5 * k]);
+        for (int k = 0; k < K; ++k) plan.pool.push_back(qs[5 * k] / (1.0 + qs[5 * k] * qs[5 * k]));
         for (int side = 0; side < 2; ++side) {
           for (int sub = 1; sub < (1 << K); ++sub) {
             double pr = 1.0, pi = 0.0;
             for (int k = 0; k < K; ++k) {
               if (!((sub >> k) & 1)) continue;
               const double er = qs[5 * k + 1 + 2 * side], ei = qs[5 * k + 2 + 2 * side];
-              const double nr = pr * er - pi * ei, ni = pr * ei + pi * er;
+              double nr = pr * er - pi * ei, ni = pr * ei + pi * er;
+              if (side == 0) {
+                const double f = 1.0 + qs[5 * k] * qs[5 * k];
+                nr *= f;
+                ni *= f;
+              }
               pr = nr;
               pi = ni;
             }
@@ -954,6 +988,19 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             plan.pool.push_back(pi);
           }
         }
+        sg.code = sw_code(sg.kind, sg.a, sg.b);
+        plan.gates.push_back(sg);
+        for (int i : part) plan.gate_ops.push_back(run_ops[i]);
+      };
+      // lifted-rotation record (phase-free plans) for the gates of `part`
+      // (increasing register bit), lifting shears in `qs`
+      auto emit_lifted = [&](const std::vector<int>& part, const std::vector<double>& qs) {
+        SwGate sg;
+        std::memset(&sg, 0, sizeof sg);
+        sg.moff = (int32_t)plan.pool.size();
+        sg.kind = SK_ROTL;
+        for (int i : part) sg.a |= 1 << run[i].first;
+        plan.pool.insert(plan.pool.end(), qs.begin(), qs.end());
         sg.code = sw_code(sg.kind, sg.a, sg.b);
         plan.gates.push_back(sg);
         for (int i : part) plan.gate_ops.push_back(run_ops[i]);
@@ -984,6 +1031,22 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
         std::sort(order.begin(), order.end(), [&](int x, int y) { return run[x].first < run[y].first; });
         std::vector<int> rot, mat, xrot;
         std::vector<double> qs;
+        if (pp.phase_free) {
+          for (int i : order) {
+            double q[2];
+            if (lifted_rotation(run[i].second, q)) {
+              rot.push_back(i);
+              qs.insert(qs.end(), q, q + 2);
+            } else {
+              mat.push_back(i);
+            }
+          }
+          if (!rot.empty()) emit_lifted(rot, qs);
+          if (!mat.empty()) emit_matrix(mat);
+          run.clear();
+          run_ops.clear();
+          return;
+        }
         double sr = sw.scale_re, si = sw.scale_im;
         for (int i : order) {
           double q[5], fr, fi;
@@ -1121,6 +1184,20 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
             if (pg.cmask == 0 && sg.a >= 0 && reg_of_pos[sg.a] >= 0) {
               sg.kind = SK_D1R;
               sg.a = reg_of_pos[sg.a];
+              const double n0 = pg.m[0] * pg.m[0] + pg.m[1] * pg.m[1];
+              if (pp.phase_free && n0 > 0.0) {
+                // diag(d0, d1) = d0 diag(1, d1 / d0); the phase-free plan keeps the second
+                sg.kind = SK_D1H;
+                const double dr = (pg.m[2] * pg.m[0] + pg.m[3] * pg.m[1]) / n0;
+                const double di = (pg.m[3] * pg.m[0] - pg.m[2] * pg.m[1]) / n0;
+                // |d0| = 1 for the unitaries of a gradient plan; anything else keeps d0
+                if (std::fabs(n0 - 1.0) <= 1e-13) {
+                  plan.pool.push_back(dr);
+                  plan.pool.push_back(di);
+                  break;
+                }
+                sg.kind = SK_D1R;
+              }
             }
             plan.pool.insert(plan.pool.end(), pg.m, pg.m + 4);
             break;

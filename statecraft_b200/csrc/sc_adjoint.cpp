@@ -114,7 +114,8 @@ int reserve_scratch(Ctx* c, int64_t n_params) {
 }
 
 // Sweep shape of the reverse pass: 3 register qubits (both states' registers in one
-// thread), plain matrix records; 2048-amplitude tiles (256 threads) unless
+// thread), phase-free records (lifted rotations, half diagonals) and plain matrix
+// records; 2048-amplitude tiles (256 threads) unless
 // STATECRAFT_B200_ADJOINT_TILE sets the tile qubits (10: 128-thread tiles).
 PlanParams reverse_plan_params(const Ctx* c) {
   PlanParams pp;
@@ -132,6 +133,9 @@ PlanParams reverse_plan_params(const Ctx* c) {
   pp.relayout = false;
   pp.rot_min_c = 0.0;
   pp.peephole = false;
+  // both states take every gate: phases common to a gate cancel in the probes, so
+  // real rotations run as lifting shears and 1-qubit diagonals as diag(1, d)
+  pp.phase_free = true;
   return pp;
 }
 

@@ -237,7 +237,7 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
               int bits[8], K = 0;
               for (int bit = 0; bit < NR; ++bit)
                 if ((g.a >> bit) & 1) bits[K++] = bit;
-              const double* lam = m + K;
+              const double* lam = m + 2 * K;
               const double* phi = lam + 2 * ((1 << K) - 1);
               auto subset = [&](int j) {
                 int sub = 0;
@@ -251,13 +251,16 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
               for (int j = 0; j < NV; ++j)
                 if (const int sub = subset(j)) v[j] = cm(lam[2 * (sub - 1)], lam[2 * (sub - 1) + 1], v[j]);
               for (int k = 0; k < K; ++k) {
-                const double t = m[k];
+                // the input table scaled the 1 side by 1 + t^2: two shears
+                const double t = m[k], tp = m[K + k];
                 for (int j = 0; j < NV; ++j) {
                   if (j & (1 << bits[k])) continue;
                   const int j1 = j | (1 << bits[k]);
-                  const C a0 = v[j], a1 = v[j1];
-                  v[j] = {a0.r - t * a1.r, a0.i - t * a1.i};
-                  v[j1] = {t * a0.r + a1.r, t * a0.i + a1.i};
+                  C a0 = v[j];
+                  const C a1 = v[j1];
+                  a0 = {std::fma(-tp, a1.r, a0.r), std::fma(-tp, a1.i, a0.i)};
+                  v[j] = a0;
+                  v[j1] = {std::fma(t, a0.r, a1.r), std::fma(t, a0.i, a1.i)};
                 }
               }
               for (int j = 0; j < NV; ++j)

@@ -76,7 +76,9 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        applies i^p X^u Z^w over the register bits (u, w bit masks).
 // SK_G1ALLQ: SK_G1ALL in rotation form: each 2x2 unitary is s_g * diag(1, e^{i phi})
 //        [[1, -t], [t, 1]] diag(1, e^{i lam}).  Pool: t of each of the K gates, then
-//        the products of their e^{i lam} and of their e^{i phi} over every non-empty
+//        t / (1 + t^2) of each, then the products of their (1 + t^2) e^{i lam}
+//        (the real factor makes each rotation two in-place shears) and of their
+//        e^{i phi} over every non-empty
 //        subset of the gates (2 x (2^K - 1) complex; bit k of the subset index is the
 //        k-th gate in increasing register bit).  The scalars s_g are carried in
 //        SwSweep::scale and applied to every amplitude at a sweep's store.  b: register
@@ -93,9 +95,16 @@ bool normalise_op(const sc_op& op, const double* params, int64_t n_params, PGate
 //        diagonals of a stage merged into one record.
 // SK_TMAT: 2x2 matrix on register bit a read per trajectory from the batch's matrix
 //        table (b = Kraus point: entry b * batch + trajectory, 8 reals).
+// SK_ROTL: real rotations [[cos al, -sin al], [sin al, cos al]] on the register bits of
+//        mask a (plans whose global phase is free, PlanParams::phase_free), each as
+//        three in-place shears a0 += p a1, a1 += s a0, a0 += p a1 with p = -tan(al/2),
+//        s = sin al, |al| <= pi/2.  Pool: (p, s) per gate in increasing register bit.
+// SK_D1H: diag(1, d) on register bit a (a 1-qubit diagonal with its global phase
+//        dropped, phase-free plans); pool: d (complex).
 enum SwKind : int32_t {
   SK_G1 = 0, SK_G2, SK_X, SK_SWAP, SK_D1, SK_D2, SK_DP, SK_CX, SK_DPR, SK_G1ALL, SK_D1R,
-  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF, SK_DTAB, SK_TMAT
+  SK_X0, SK_CX0, SK_PAULI, SK_G1ALLQ, SK_XF, SK_CXF, SK_PROBE, SK_PAULIF, SK_DTAB, SK_TMAT,
+  SK_ROTL, SK_D1H
 };
 
 // Dispatch code of a sweep gate: kind << 4 | a << 2 | b for kinds whose a / b are
@@ -104,10 +113,12 @@ enum SwKind : int32_t {
 inline int32_t sw_code(int32_t kind, int32_t a, int32_t b) {
   switch (kind) {
     case SK_G1: case SK_X: case SK_D1R: case SK_X0: case SK_PAULI: case SK_XF: case SK_TMAT:
+    case SK_D1H:
       return (kind << 4) | (a << 2);
     case SK_G2: case SK_SWAP: case SK_CX: case SK_DPR: case SK_CX0: case SK_CXF:
       return (kind << 4) | (a << 2) | b;
-    case SK_G1ALL: case SK_G1ALLQ: return (kind << 4) | (a & 15);  // a = register-bit mask
+    case SK_G1ALL: case SK_G1ALLQ: case SK_ROTL:
+      return (kind << 4) | (a & 15);  // a = register-bit mask
     default: return kind << 4;
   }
 }
@@ -186,6 +197,11 @@ struct PlanParams {
   double scale_floor = 0x1p-200;
   // per-stage record peephole (diagonals merged or moved, permutations folded)
   bool peephole = true;
+  // a common phase of the whole state may be dropped: the adjoint reverse pass
+  // applies every gate to both of its states, so a phase e^{ig} (or a sign) on a
+  // gate cancels in every probe Im <lambda| P |psi>.  1-qubit real rotations up to
+  // a phase become SK_ROTL records and 1-qubit diagonals on register bits SK_D1H.
+  bool phase_free = false;
 };
 
 // matrix reals a normalised gate stores in the sweep pool

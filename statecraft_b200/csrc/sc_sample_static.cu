@@ -24,7 +24,8 @@
 // Every call shares the array and it keeps the previous call's contents; the
 // kernels write every word they read earlier in the same call, so nothing needs
 // clearing, but calls that overlap on the GPU race on the array.  Each call waits
-// for its stream and reads a status word back before it returns.
+// for its stream and reads a status word back before it returns, so a call on a
+// stream that is capturing returns SC_EINVAL before it enqueues anything.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -80,8 +81,17 @@ extern "C" int32_t sc_sample_static(const void* d_state, int32_t n_qubits, int32
     return fail(SC_EINVAL, "sc_sample_static supports states of up to 2^30 amplitudes (30 qubits), got %d qubits",
                 n_qubits);
   if (shots <= 0) return fail(SC_EINVAL, "shots must be positive");
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the call ends by waiting for the stream, which a capturing stream does not
+  // allow (and the wait would invalidate the caller's capture): refuse before any
+  // work is enqueued or the scratch array is looked up
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaError_t e = cudaStreamIsCapturing(s, &cap);
+  if (e != cudaSuccess) return fail_cuda(e, "cudaStreamIsCapturing");
+  if (cap != cudaStreamCaptureStatusNone)
+    return fail(SC_EINVAL, "sc_sample_static waits for its stream and cannot be called while the stream is capturing");
   int device = 0;
-  cudaError_t e = cudaGetDevice(&device);
+  e = cudaGetDevice(&device);
   if (e != cudaSuccess) return fail_cuda(e, "cudaGetDevice");
   if (device < 0 || device >= kMaxDevices) return fail(SC_EINVAL, "device ordinal %d out of range", device);
   double* scratch = nullptr;
@@ -90,7 +100,6 @@ extern "C" int32_t sc_sample_static(const void* d_state, int32_t n_qubits, int32
   int sms = 148;
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device)) != cudaSuccess)
     return fail_cuda(e, "cudaDeviceGetAttribute");
-  cudaStream_t s = static_cast<cudaStream_t>(stream);
   SampleArgs a;
   a.chunk_sums = scratch;
   a.chunk_prefix = scratch + kStaticChunks;

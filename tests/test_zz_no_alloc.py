@@ -73,3 +73,38 @@ def test_static_sampler_rejects_oversized_state():
                                   ctypes.c_void_p(16), None)
         assert rc == A.SC_EINVAL
         assert b"2^30" in lib.sc_last_error()
+
+
+def test_static_sampler_refuses_capturing_stream():
+    """A call on a stream that is recording a CUDA graph returns SC_EINVAL and
+    enqueues nothing: it would end by waiting for the stream, which a capturing
+    stream does not allow.  The caller's capture stays valid and replays."""
+    import torch
+
+    lib = A.load()
+    n, shots = 10, 8
+    state = torch.zeros(2 << n, dtype=torch.float64, device="cuda")
+    state[0] = 1.0
+    d_out = torch.full((shots,), -1, dtype=torch.int32, device="cuda")
+    x = torch.zeros(4, device="cuda")
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        g.capture_begin()
+        x.add_(1)
+        rc = lib.sc_sample_static(ctypes.c_void_p(state.data_ptr()), n, A.SC_C128, shots, 3, None,
+                                  ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+        x.add_(1)
+        g.capture_end()
+    assert rc == A.SC_EINVAL
+    assert b"capturing" in lib.sc_last_error()
+    g.replay()
+    torch.cuda.synchronize()
+    assert x.tolist() == [2.0] * 4
+    assert d_out.tolist() == [-1] * shots
+    # the same buffers sample normally once the capture is over
+    rc = lib.sc_sample_static(ctypes.c_void_p(state.data_ptr()), n, A.SC_C128, shots, 3, None,
+                              ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(s.cuda_stream))
+    A.raise_for(rc, lib)
+    assert d_out.tolist() == [0] * shots
