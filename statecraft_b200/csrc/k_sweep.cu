@@ -110,52 +110,6 @@ __device__ __forceinline__ void g1(typename Amp<R>::type (&v)[1 << NR], const R*
   }
 }
 
-template <typename R, int NR, int A_>
-__device__ __forceinline__ void xswap(typename Amp<R>::type (&v)[1 << NR], uint32_t l0,
-                                      const RegOff<NR>& off, uint32_t lmask) {
-  if (lmask == 0) {  // no control inside the tile: a plain register permutation
-#pragma unroll
-    for (int j = 0; j < (1 << NR); ++j) {
-      if (j & (1 << A_)) continue;
-      const auto t = v[j];
-      v[j] = v[j | (1 << A_)];
-      v[j | (1 << A_)] = t;
-    }
-    return;
-  }
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) {
-    if (j & (1 << A_)) continue;
-    const int j1 = j | (1 << A_);
-    const bool on = ((l0 | off[j]) & lmask) == lmask;
-    const auto a0 = v[j], a1 = v[j1];
-    v[j] = on ? a1 : a0;
-    v[j1] = on ? a0 : a1;
-  }
-}
-
-// controlled X with target register bit T_ and control register bit C_; further
-// controls (lmask) lie on tile positions outside the registers, so their test is
-// the same for all of a thread's registers
-template <typename R, int NR, int T_, int C_>
-__device__ __forceinline__ void cxswap(typename Amp<R>::type (&v)[1 << NR], uint32_t l0,
-                                       uint32_t lmask) {
-  const bool on = (l0 & lmask) == lmask;
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) {
-    if ((j & (1 << T_)) || !(j & (1 << C_))) continue;
-    const int j1 = j | (1 << T_);
-    const auto a0 = v[j], a1 = v[j1];
-    if (lmask == 0) {
-      v[j] = a1;
-      v[j1] = a0;
-    } else {
-      v[j] = on ? a1 : a0;
-      v[j1] = on ? a0 : a1;
-    }
-  }
-}
-
 // parity diagonal on register bits A_, B_: factor d[bit A_ ^ bit B_], fixed per register
 template <typename R, int NR, int A_, int B_>
 __device__ __forceinline__ void dpr(typename Amp<R>::type (&v)[1 << NR], const R* m) {
@@ -191,18 +145,6 @@ __device__ __forceinline__ void g2(typename Amp<R>::type (&v)[1 << NR], const R*
       }
       v[idx[r]] = o;
     }
-  }
-}
-
-template <typename R, int NR, int A_, int B_>
-__device__ __forceinline__ void rswap(typename Amp<R>::type (&v)[1 << NR]) {
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) {
-    if (j & ((1 << A_) | (1 << B_))) continue;
-    const int ja = j | (1 << A_), jb = j | (1 << B_);
-    const auto t = v[ja];
-    v[ja] = v[jb];
-    v[jb] = t;
   }
 }
 
@@ -259,38 +201,6 @@ __device__ __forceinline__ void diag2_any(typename Amp<R>::type (&v)[1 << NR], c
   }
 }
 
-template <int NR, typename F>
-__device__ __forceinline__ void dispatch1(int a, F&& f) {
-  switch (a) {
-    case 0: f(std::integral_constant<int, 0>()); break;
-    case 1: if constexpr (NR > 1) f(std::integral_constant<int, 1>()); break;
-    case 2: if constexpr (NR > 2) f(std::integral_constant<int, 2>()); break;
-    case 3: if constexpr (NR > 3) f(std::integral_constant<int, 3>()); break;
-    default: break;
-  }
-}
-
-template <int NR, typename F>
-__device__ __forceinline__ void dispatch2(int a, int b, F&& f) {
-  dispatch1<NR>(a, [&](auto ia) {
-    dispatch1<NR>(b, [&](auto ib) {
-      if constexpr (decltype(ia)::value != decltype(ib)::value) f(ia, ib);
-    });
-  });
-}
-
-// X on register bit A_ with no tile controls outside the registers
-template <typename R, int NR, int A_>
-__device__ __forceinline__ void xswap0(typename Amp<R>::type (&v)[1 << NR]) {
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) {
-    if (j & (1 << A_)) continue;
-    const auto t = v[j];
-    v[j] = v[j | (1 << A_)];
-    v[j | (1 << A_)] = t;
-  }
-}
-
 // X on register bit A_ applied to the stage's exit slots: the amplitude in register
 // j leaves through the slot of register j ^ (1 << A_), whose swizzled offset differs
 // by m = xoff[A_], the slot offset of that bit (the offsets are linear in j); m = 0 where the gate's
@@ -304,18 +214,6 @@ __device__ __forceinline__ void xfold(SlotFlips<NR>& fl, uint32_t m) {
 template <int NR, int T_, int C_>
 __device__ __forceinline__ void cxfold(SlotFlips<NR>& fl, uint32_t m) {
   fl.xc[C_] ^= m;
-}
-
-// controlled X, target register bit T_, control register bit C_, no other tile controls
-template <typename R, int NR, int T_, int C_>
-__device__ __forceinline__ void cxswap0(typename Amp<R>::type (&v)[1 << NR]) {
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) {
-    if ((j & (1 << T_)) || !(j & (1 << C_))) continue;
-    const auto t = v[j];
-    v[j] = v[j | (1 << T_)];
-    v[j | (1 << T_)] = t;
-  }
 }
 
 // uncontrolled diag(d0, d1) on register bit A_: the factor of each register is fixed
@@ -405,73 +303,6 @@ __device__ __forceinline__ void g1all(typename Amp<R>::type (&v)[1 << NR], const
   if constexpr (NR > 3 && (M & 8) != 0) g1<R, NR, 3>(v, mm, l0, off, 0u);
 }
 
-// Pauli chosen per trajectory on register bit A_: 1 = X, 2 = Y, 3 = Z (the
-// identity never reaches here)
-template <typename R, int NR, int A_>
-__device__ __forceinline__ void pauli(typename Amp<R>::type (&v)[1 << NR], uint32_t code) {
-  const bool flip = code != 3u;                  // X, Y swap the pair
-  const R s0 = code == 2u ? (R)-1 : (R)1;        // Y: new0 = -i a1, new1 = i a0
-  const R s1 = code == 1u ? (R)1 : (R)-1;        // Z: new1 = -a1
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j) {
-    if (j & (1 << A_)) continue;
-    const int j1 = j | (1 << A_);
-    const auto a0 = v[j], a1 = v[j1];
-    if (code == 2u) {
-      v[j] = make_amp<R>(a1.y, s0 * a1.x);
-      v[j1] = make_amp<R>(-a0.y, a0.x);
-    } else {
-      v[j] = flip ? a1 : a0;
-      const auto b = flip ? a0 : a1;
-      v[j1] = make_amp<R>(s1 * b.x, s1 * b.y);
-    }
-  }
-}
-
-// Pauli slot conjugated through folded register permutations: i^p X^u Z^w over the
-// register bits, f = (u, w, p) of the trajectory's choice
-template <typename R, int NR>
-__device__ __forceinline__ void pauli_frame(typename Amp<R>::type (&v)[1 << NR], const R* f) {
-  const uint32_t u = (uint32_t)f[0], w = (uint32_t)f[1], ph = (uint32_t)f[2];
-#pragma unroll
-  for (int j = 0; j < (1 << NR); ++j)
-    if (__popc(w & (uint32_t)j) & 1) v[j] = make_amp<R>(-v[j].x, -v[j].y);
-  if (u & 1u) xswap0<R, NR, 0>(v);
-  if constexpr (NR > 1) {
-    if (u & 2u) xswap0<R, NR, 1>(v);
-  }
-  if constexpr (NR > 2) {
-    if (u & 4u) xswap0<R, NR, 2>(v);
-  }
-  if constexpr (NR > 3) {
-    if (u & 8u) xswap0<R, NR, 3>(v);
-  }
-  if (ph & 1u) {
-#pragma unroll
-    for (int j = 0; j < (1 << NR); ++j) v[j] = make_amp<R>(-v[j].y, v[j].x);
-  }
-  if (ph & 2u) {
-#pragma unroll
-    for (int j = 0; j < (1 << NR); ++j) v[j] = make_amp<R>(-v[j].x, -v[j].y);
-  }
-}
-
-// X on the register bits of mask b (a rotation record's leading X, when it is not
-// folded into the stage's read)
-template <typename R, int NR>
-__device__ __forceinline__ void prex(typename Amp<R>::type (&v)[1 << NR], uint32_t b) {
-  if (b & 1u) xswap0<R, NR, 0>(v);
-  if constexpr (NR > 1) {
-    if (b & 2u) xswap0<R, NR, 1>(v);
-  }
-  if constexpr (NR > 2) {
-    if (b & 4u) xswap0<R, NR, 2>(v);
-  }
-  if constexpr (NR > 3) {
-    if (b & 8u) xswap0<R, NR, 3>(v);
-  }
-}
-
 // real rotations on the register bits of mask M as lifting shears (pool: p, s per
 // bit, ascending): a0 += p a1, a1 += s a0, a0 += p a1, every update in place
 template <typename R, int NR, int M>
@@ -509,6 +340,79 @@ template <typename R, int NR>
 __device__ __forceinline__ void dtab(typename Amp<R>::type (&v)[1 << NR], const R* m) {
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j) v[j] = cmul(m[2 * j], m[2 * j + 1], v[j]);
+}
+
+// A register permutation applied through the thread's own shared-memory slots:
+// register j goes out to the slot it was read from in this stage (rbase ^ rd[j])
+// and comes back from the slot of its source register, rbase ^ src_rd(j) (the rd
+// entry of the source; conditions select between entries, so every constant load
+// has an index common to the warp).  The slots belong to this thread alone from the
+// stage's read to the next exchange, so no barrier is needed.  Done in registers, a
+// permutation chosen at run time makes the record's code move the amplitude
+// registers back into place where the record loop joins.
+template <typename A, int NV, typename F>
+__device__ __forceinline__ void smem_permute(A (&v)[NV], A* cur, uint32_t rbase,
+                                             const SwStageTab& tab, F&& src_rd) {
+#pragma unroll
+  for (int j = 0; j < NV; ++j) cur[rbase ^ tab.rd[j]] = v[j];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ (uint32_t)src_rd(j)];
+}
+
+// Pauli chosen per trajectory on register bit A_ (1 = X, 2 = Y, 3 = Z; the identity
+// never reaches here).  Z negates in place; X and Y move the pair through the
+// thread's own slots (smem_permute), Y taking the components crosswise on the way
+// back: new0 = -i a1 = (a1.y, -a1.x), new1 = i a0 = (-a0.y, a0.x).
+template <typename R, int NR, int A_>
+__device__ __forceinline__ void pauli_slots(typename Amp<R>::type (&v)[1 << NR], uint32_t code,
+                                            typename Amp<R>::type* cur, uint32_t rbase,
+                                            const SwStageTab& tab) {
+  if (code == 3u) {
+#pragma unroll
+    for (int j = 0; j < (1 << NR); ++j)
+      if ((j >> A_) & 1) v[j] = make_amp<R>(-v[j].x, -v[j].y);
+    return;
+  }
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) cur[rbase ^ tab.rd[j]] = v[j];
+  const uint32_t c = code == 2u ? 1u : 0u;  // Y: components crosswise
+  const R sg = code == 2u ? (R)-1 : (R)1;
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const R* sp = reinterpret_cast<const R*>(cur + (rbase ^ tab.rd[j ^ (1 << A_)]));
+    const R c0 = sp[c], c1 = sp[c ^ 1u];
+    if ((j >> A_) & 1) {
+      v[j].x = sg * c0;
+      v[j].y = c1;
+    } else {
+      v[j].x = c0;
+      v[j].y = sg * c1;
+    }
+  }
+}
+
+// Pauli slot conjugated through folded register permutations: i^p X^u Z^w over the
+// register bits, f = (u, w, p) of the trajectory's choice.  Register j takes
+// i^p (-1)^{|w & (j ^ u)|} times register j ^ u, through the thread's own slots (the
+// i^p taken as a component swap and signs on the way back).
+template <typename R, int NR>
+__device__ __forceinline__ void pauli_frame_slots(typename Amp<R>::type (&v)[1 << NR], const R* f,
+                                                  typename Amp<R>::type* cur, uint32_t rbase,
+                                                  const SwStageTab& tab) {
+  const uint32_t u = (uint32_t)f[0], w = (uint32_t)f[1], ph = (uint32_t)f[2] & 3u;
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) cur[rbase ^ tab.rd[j]] = v[j];
+  const uint32_t c = ph & 1u;  // odd powers of i swap the components
+  const R sx = (ph == 1u || ph == 2u) ? (R)-1 : (R)1;
+  const R sy = (ph >= 2u) ? (R)-1 : (R)1;
+#pragma unroll
+  for (int j = 0; j < (1 << NR); ++j) {
+    const uint32_t src = ((uint32_t)j ^ u) & ((1u << NR) - 1u);
+    const R* sp = reinterpret_cast<const R*>(cur + (rbase ^ tab.rd[src]));
+    const R sw = (__popc(w & src) & 1) ? (R)-1 : (R)1;
+    v[j].x = (sx * sw) * sp[c];
+    v[j].y = (sy * sw) * sp[c ^ 1u];
+  }
 }
 
 // switch cases for the dispatch code (sw_code): one jump per gate into code that
@@ -732,12 +636,26 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
       }
     }
 
+    // the read flip of a stage's conditional entry folds, for the thread's stage base
+    auto entry_flip = [&](const SwStageTab& tab, uint32_t lbase) -> uint32_t {
+      uint32_t f = 0;
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        if (tab.rf_g[k] < 0) continue;
+        const SwGate& q = p.gates[tab.rf_g[k]];
+        if (((uint64_t)base & q.gmask) == q.gmask && (lbase & q.lmask) == q.lmask) f ^= tab.rf_off[k];
+      }
+      return f;
+    };
     A v[NV];
+    // the thread's read base in the current stage: its slots are rbase ^ rd[j]
+    uint32_t rbase;
     {
       // both copy paths leave the tile in `cur` in the linear layout
       const SwStageTab& tab = p.tabs[0];
+      rbase = l0_first ^ entry_flip(tab, l0_first);
 #pragma unroll
-      for (int j = 0; j < NV; ++j) v[j] = cur[l0_first ^ tab.rd[j]];
+      for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
     }
     uint32_t l0 = l0_first, psw0 = 0;
     RegOff<NR> off;
@@ -755,9 +673,9 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
 #pragma unroll
         for (int j = 0; j < NV; ++j) cur[psw0 ^ ptab.wsoff[j] ^ sidx[j]] = v[j];
         __syncthreads();
-        const uint32_t sw0 = stage_swz<R>(nl0, tab);
+        rbase = stage_swz<R>(nl0, tab) ^ entry_flip(tab, nl0);
 #pragma unroll
-        for (int j = 0; j < NV; ++j) v[j] = cur[sw0 ^ tab.rd[j]];
+        for (int j = 0; j < NV; ++j) v[j] = cur[rbase ^ tab.rd[j]];
       }
       // this stage's exit slots are in the next stage's layout
       psw0 = s + 1 < ns ? stage_swz<R>(nl0, p.tabs[s + 1]) : 0u;
@@ -793,17 +711,27 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
         const uint32_t lmask = g.lmask;
         switch (g.code) {
 #define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask)
-#define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask)
+#define SC_DO_X(A)                                                                        \
+  smem_permute(v, cur, rbase, tab, [&](int j) {                                           \
+    return (((l0 | off[j]) & lmask) == lmask) ? tab.rd[j ^ (1 << (A))] : tab.rd[j];       \
+  })
 #define SC_DO_D1R(A) d1r<R, NR, A>(v, m)
 #define SC_DO_G2(A, B) g2<R, NR, A, B>(v, m)
-#define SC_DO_CX(A, B) cxswap<R, NR, A, B>(v, l0, lmask)
+#define SC_DO_CX(A, B)                                                                    \
+  smem_permute(v, cur, rbase, tab, [&](int j) {                                           \
+    return (((j >> (B)) & 1) && (l0 & lmask) == lmask) ? tab.rd[j ^ (1 << (A))] : tab.rd[j]; \
+  })
 #define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m)
-#define SC_DO_SWAP(A, B) rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v)
-#define SC_DO_X0(A) xswap0<R, NR, A>(v)
-#define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v)
-#define SC_DO_PAULI(A)                        \
-  if constexpr (kBatch) {                     \
-    pauli<R, NR, A>(v, (uint32_t)codes[g.b]); \
+#define SC_DO_SWAP(A, B)                                                                  \
+  smem_permute(v, cur, rbase, tab, [&](int j) {                                           \
+    return tab.rd[(((j >> (A)) ^ (j >> (B))) & 1) ? j ^ ((1 << (A)) | (1 << (B))) : j];    \
+  })
+#define SC_DO_X0(A) smem_permute(v, cur, rbase, tab, [&](int j) { return tab.rd[j ^ (1 << (A))]; })
+#define SC_DO_CX0(A, B) \
+  smem_permute(v, cur, rbase, tab, [&](int j) { return tab.rd[((j >> (B)) & 1) ? j ^ (1 << (A)) : j]; })
+#define SC_DO_PAULI(A)                                                   \
+  if constexpr (kBatch) {                                                \
+    pauli_slots<R, NR, A>(v, (uint32_t)codes[g.b], cur, rbase, tab);     \
   }
 #define SC_DO_XF(A) \
   xfold<NR, A>(sidx, (l0 & lmask) == lmask ? (uint32_t)tab.xoff[A] : 0u)
@@ -825,7 +753,7 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
 #undef SC_DO_TMAT
           case SK_PAULIF << 4:
             if constexpr (kBatch) {
-              pauli_frame<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u));
+              pauli_frame_slots<R, NR>(v, m + 3 * ((uint32_t)codes[g.b] - 1u), cur, rbase, tab);
             }
             break;
 #undef SC_DO_X0
@@ -861,7 +789,10 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
 #define SC_G1ALLQ_CASE(M)                                   \
   case (SK_G1ALLQ << 4) | (M):                              \
     if constexpr (((M) >> NR) == 0) {                       \
-      if (g.b && !folded_x) prex<R, NR>(v, (uint32_t)g.b);  \
+      if (g.b && !folded_x) {                               \
+        const int xb = g.b & (NV - 1);                      \
+        smem_permute(v, cur, rbase, tab, [&](int j) { return tab.rd[j ^ xb]; }); \
+      }                                                     \
       g1allq<R, NR, (M)>(v, m);                             \
     }                                                       \
     break;
@@ -914,45 +845,52 @@ __global__ void __launch_bounds__(sweep_max_threads<R, NR>())
 // shared slot per warp -> per-CTA partial, and are added up in a fixed order.
 // ---------------------------------------------------------------------------
 
-// A record of an adjoint plan (1-qubit matrix records, permutations, diagonals;
-// plans with dense 2-qubit records take the gate-by-gate path) applied to both
-// states in one dispatch: one join of the register state per record, not two.
+// Records of the adjoint plan outside the lite set (kLite below): register
+// permutations (X, CNOT, SWAP) not folded into a stage's read, 2-qubit diagonals,
+// grouped 1-qubit matrices, diagonal tables, diagonals whose bits lie outside the
+// registers.
 template <typename R, int NR>
-__device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 << NR],
-                                                  typename Amp<R>::type (&w)[1 << NR],
-                                                  const SwGate& g, const R* m, uint32_t l0,
-                                                  const RegOff<NR>& off, uint32_t base) {
+__device__ __forceinline__ void apply_record_pair_rest(typename Amp<R>::type (&v)[1 << NR],
+                                                       typename Amp<R>::type (&w)[1 << NR],
+                                                       const SwGate& g, const R* m, uint32_t l0,
+                                                       const RegOff<NR>& off, uint32_t base,
+                                                       typename Amp<R>::type* bp,
+                                                       typename Amp<R>::type* bl, uint32_t rbase,
+                                                       const SwStageTab& tab) {
   const uint32_t lmask = g.lmask;
+  // register permutations go through the thread's own slots of both tile buffers
+  auto perm2 = [&](auto&& src_rd) {
+    smem_permute(v, bp, rbase, tab, src_rd);
+    smem_permute(w, bl, rbase, tab, src_rd);
+  };
   switch (g.code) {
-#define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask), g1<R, NR, A>(w, m, l0, off, lmask)
-#define SC_DO_X(A) xswap<R, NR, A>(v, l0, off, lmask), xswap<R, NR, A>(w, l0, off, lmask)
-#define SC_DO_D1R(A) d1r<R, NR, A>(v, m), d1r<R, NR, A>(w, m)
-#define SC_DO_CX(A, B) cxswap<R, NR, A, B>(v, l0, lmask), cxswap<R, NR, A, B>(w, l0, lmask)
-#define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m), dpr<R, NR, A, B>(w, m)
-#define SC_DO_SWAP(A, B)                                          \
-  rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(v), \
-      rswap<R, NR, ((A) < (B) ? (A) : (B)), ((A) < (B) ? (B) : (A))>(w)
-#define SC_DO_X0(A) xswap0<R, NR, A>(v), xswap0<R, NR, A>(w)
-#define SC_DO_CX0(A, B) cxswap0<R, NR, A, B>(v), cxswap0<R, NR, A, B>(w)
-#define SC_DO_D1H(A) d1h<R, NR, A>(v, m), d1h<R, NR, A>(w, m)
-    SC_CASES_1(SK_D1H, SC_DO_D1H)
-#undef SC_DO_D1H
-    SC_CASES_1(SK_G1, SC_DO_G1)
+#define SC_DO_X(A)                                                                          \
+  perm2([&](int j) {                                                                        \
+    return (((l0 | off[j]) & lmask) == lmask) ? tab.rd[j ^ (1 << (A))] : tab.rd[j];         \
+  })
+#define SC_DO_CX(A, B)                                                                      \
+  perm2([&](int j) {                                                                        \
+    return (((j >> (B)) & 1) && (l0 & lmask) == lmask) ? tab.rd[j ^ (1 << (A))] : tab.rd[j]; \
+  })
+#define SC_DO_X0(A) perm2([&](int j) { return tab.rd[j ^ (1 << (A))]; })
+#define SC_DO_CX0(A, B) perm2([&](int j) { return tab.rd[((j >> (B)) & 1) ? j ^ (1 << (A)) : j]; })
     SC_CASES_1(SK_X, SC_DO_X)
-    SC_CASES_1(SK_D1R, SC_DO_D1R)
     SC_CASES_2(SK_CX, SC_DO_CX)
-    SC_CASES_2(SK_DPR, SC_DO_DPR)
-    SC_CASES_2(SK_SWAP, SC_DO_SWAP)
     SC_CASES_1(SK_X0, SC_DO_X0)
     SC_CASES_2(SK_CX0, SC_DO_CX0)
-#undef SC_DO_G1
 #undef SC_DO_X
-#undef SC_DO_D1R
 #undef SC_DO_CX
-#undef SC_DO_DPR
-#undef SC_DO_SWAP
 #undef SC_DO_X0
 #undef SC_DO_CX0
+#define SC_DO_DPR(A, B) dpr<R, NR, A, B>(v, m), dpr<R, NR, A, B>(w, m)
+#define SC_DO_SWAP(A, B)                                                                    \
+  perm2([&](int j) {                                                                        \
+    return tab.rd[(((j >> (A)) ^ (j >> (B))) & 1) ? j ^ ((1 << (A)) | (1 << (B))) : j];     \
+  })
+    SC_CASES_2(SK_DPR, SC_DO_DPR)
+    SC_CASES_2(SK_SWAP, SC_DO_SWAP)
+#undef SC_DO_DPR
+#undef SC_DO_SWAP
 #define SC_G1ALL_CASE(M)                        \
   case (SK_G1ALL << 4) | (M):                   \
     if constexpr (((M) >> NR) == 0) {           \
@@ -965,16 +903,6 @@ __device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 <
     SC_G1ALL_CASE(9) SC_G1ALL_CASE(10) SC_G1ALL_CASE(11) SC_G1ALL_CASE(12)
     SC_G1ALL_CASE(13) SC_G1ALL_CASE(14) SC_G1ALL_CASE(15)
 #undef SC_G1ALL_CASE
-#define SC_ROTL_CASE(M)                         \
-  case (SK_ROTL << 4) | (M):                    \
-    if constexpr (((M) >> NR) == 0) {           \
-      rotl<R, NR, (M)>(v, m);                   \
-      rotl<R, NR, (M)>(w, m);                   \
-    }                                           \
-    break;
-    SC_ROTL_CASE(1) SC_ROTL_CASE(2) SC_ROTL_CASE(3) SC_ROTL_CASE(4)
-    SC_ROTL_CASE(5) SC_ROTL_CASE(6) SC_ROTL_CASE(7)
-#undef SC_ROTL_CASE
     case SK_DTAB << 4:
       dtab<R, NR>(v, m);
       dtab<R, NR>(w, m);
@@ -995,13 +923,62 @@ __device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 <
   }
 }
 
+// A record of the adjoint plan applied to both states in one dispatch: one join of
+// the register state per record, not two.  kLite: only the records of phase-free
+// rotation plans once their register permutations are folded into the stages'
+// reads (lifted rotations, half diagonals, 1-qubit matrices, probes).  A case that
+// permutes the registers at run time, even one that never runs, makes the record
+// loop move the amplitude registers at every record's join (measured: about half
+// the instructions of the 26-qubit HEA reverse sweep); the host picks the lite
+// kernel when every record the sweep executes is of those kinds.
+template <typename R, int NR, bool kLite>
+__device__ __forceinline__ void apply_record_pair(typename Amp<R>::type (&v)[1 << NR],
+                                                  typename Amp<R>::type (&w)[1 << NR],
+                                                  const SwGate& g, const R* m, uint32_t l0,
+                                                  const RegOff<NR>& off, uint32_t base,
+                                                  typename Amp<R>::type* bp,
+                                                  typename Amp<R>::type* bl, uint32_t rbase,
+                                                  const SwStageTab& tab) {
+  const uint32_t lmask = g.lmask;
+  switch (g.code) {
+#define SC_DO_G1(A) g1<R, NR, A>(v, m, l0, off, lmask), g1<R, NR, A>(w, m, l0, off, lmask)
+#define SC_DO_D1R(A) d1r<R, NR, A>(v, m), d1r<R, NR, A>(w, m)
+#define SC_DO_D1H(A) d1h<R, NR, A>(v, m), d1h<R, NR, A>(w, m)
+    SC_CASES_1(SK_D1H, SC_DO_D1H)
+    SC_CASES_1(SK_G1, SC_DO_G1)
+    SC_CASES_1(SK_D1R, SC_DO_D1R)
+#undef SC_DO_D1H
+#undef SC_DO_G1
+#undef SC_DO_D1R
+#define SC_ROTL_CASE(M)                         \
+  case (SK_ROTL << 4) | (M):                    \
+    if constexpr (((M) >> NR) == 0) {           \
+      rotl<R, NR, (M)>(v, m);                   \
+      rotl<R, NR, (M)>(w, m);                   \
+    }                                           \
+    break;
+    SC_ROTL_CASE(1) SC_ROTL_CASE(2) SC_ROTL_CASE(3) SC_ROTL_CASE(4)
+    SC_ROTL_CASE(5) SC_ROTL_CASE(6) SC_ROTL_CASE(7)
+#undef SC_ROTL_CASE
+    default:
+      if constexpr (!kLite) apply_record_pair_rest<R, NR>(v, w, g, m, l0, off, base, bp, bl, rbase, tab);
+      break;
+  }
+}
+
+// the record kinds apply_record_pair<..., kLite = true> handles
+inline bool adjoint_lite_kind(int32_t k) {
+  return k == SK_ROTL || k == SK_D1H || k == SK_G1 || k == SK_D1R || k == SK_PROBE;
+}
+
 // Im sum_j conj(w_j) (P v)_j over the thread's registers, P the Pauli PAULI_
 // (1 = X, 2 = Y = iXZ, 3 = Z) on register bit A_ (the planner puts a probed
 // qubit in the registers)
 template <typename R, int NR, int A_, int PAULI_>
 __device__ __forceinline__ double probe_sum(const typename Amp<R>::type (&v)[1 << NR],
                                             const typename Amp<R>::type (&w)[1 << NR]) {
-  double s = 0.0;
+  // two partial sums (even and odd registers): half the dependent FP64 chain
+  double s[2] = {0.0, 0.0};
 #pragma unroll
   for (int j = 0; j < (1 << NR); ++j) {
     const int src = PAULI_ == 3 ? j : j ^ (1 << A_);  // X and Y move the partner in
@@ -1015,15 +992,15 @@ __device__ __forceinline__ double probe_sum(const typename Amp<R>::type (&v)[1 <
       pr = -pi;
       pi = t;
     }
-    s += (double)w[j].x * pi - (double)w[j].y * pr;
+    s[j & 1] += (double)w[j].x * pi - (double)w[j].y * pr;
   }
-  return s;
+  return s[0] + s[1];
 }
 
 // THREADS threads per tile, MINB CTAs per SM (their register cap: 65536 / (THREADS x
 // MINB)).  While a tile computes, each thread asks L2 for its amplitudes of the
 // CTA's next tile (`prefetch.global.L2`: no registers, no wait).
-template <typename R, int NR, int THREADS, int MINB>
+template <typename R, int NR, int THREADS, int MINB, bool kLite>
 __global__ void __launch_bounds__(THREADS, MINB)
     k_adjoint_sweep(typename Amp<R>::type* __restrict__ psi, typename Amp<R>::type* __restrict__ lam,
                     const __grid_constant__ SweepParams<R> p, double* __restrict__ partial,
@@ -1046,12 +1023,32 @@ __global__ void __launch_bounds__(THREADS, MINB)
   const uint32_t gt_first = spread32(l0_first, p);
   const uint32_t gt_last = spread_out32(l0_last, p);
   for (uint32_t t = blockIdx.x; t < (uint32_t)p.tiles; t += gridDim.x) {
+    // a permutation record of the full kernel works in the thread's own slots of the
+    // current stage's layout: every thread is past the last tile's final reads first
+    if constexpr (!kLite) __syncthreads();
     const uint32_t base = tile_base(t, p);
-    A v[NV], w[NV];
+    // the read flip of a stage's conditional entry folds (tab.rf_off, or the first
+    // stage's global offsets rf_goff0), for the thread's stage base
+    auto entry_flip = [&](const SwStageTab& tab, uint32_t lbase, bool global) -> uint32_t {
+      uint32_t f = 0;
 #pragma unroll
-    for (int j = 0; j < NV; ++j) {
-      v[j] = psi[base | gt_first | p.gfirst[j]];
-      w[j] = lam[base | gt_first | p.gfirst[j]];
+      for (int k = 0; k < 2; ++k) {
+        if (tab.rf_g[k] < 0) continue;
+        const SwGate& q = p.gates[tab.rf_g[k]];
+        if (((uint64_t)base & q.gmask) == q.gmask && (lbase & q.lmask) == q.lmask)
+          f ^= global ? p.rf_goff0[k] : (uint32_t)tab.rf_off[k];
+      }
+      return f;
+    };
+    A v[NV], w[NV];
+    {
+      // the flip moves register-position bits only (disjoint from base and gt_first)
+      const uint32_t gfl = entry_flip(p.tabs[0], l0_first, true);
+#pragma unroll
+      for (int j = 0; j < NV; ++j) {
+        v[j] = psi[base | gt_first | (p.gread0[j] ^ gfl)];
+        w[j] = lam[base | gt_first | (p.gread0[j] ^ gfl)];
+      }
     }
     if (t + gridDim.x < (uint32_t)p.tiles) {
       const uint32_t nb = tile_base(t + gridDim.x, p);
@@ -1061,6 +1058,8 @@ __global__ void __launch_bounds__(THREADS, MINB)
         prefetch_l2(lam + (nb | gt_first | p.gfirst[j]));
       }
     }
+    // the thread's read base in the current stage (the first stage: its linear slots)
+    uint32_t rbase = l0_first;
     uint32_t l0 = l0_first, psw0 = 0;
     RegOff<NR> off;
 #pragma unroll 1
@@ -1079,10 +1078,11 @@ __global__ void __launch_bounds__(THREADS, MINB)
           bl[psw0 ^ ptab.wsoff[j]] = w[j];
         }
         __syncthreads();
+        rbase = sw0 ^ entry_flip(tab, nl0, false);
 #pragma unroll
         for (int j = 0; j < NV; ++j) {
-          v[j] = bp[sw0 ^ tab.rd[j]];
-          w[j] = bl[sw0 ^ tab.rd[j]];
+          v[j] = bp[rbase ^ tab.rd[j]];
+          w[j] = bl[rbase ^ tab.rd[j]];
         }
       }
       psw0 = sw0;
@@ -1112,7 +1112,7 @@ __global__ void __launch_bounds__(THREADS, MINB)
           if ((tid & 31u) == 0) acc[(uint32_t)g.b * nwarps + warp] += ps;  // b: local probe index
           continue;
         }
-        apply_record_pair<R, NR>(v, w, g, p.pool + g.moff, l0, off, base);
+        apply_record_pair<R, NR, kLite>(v, w, g, p.pool + g.moff, l0, off, base, bp, bl, rbase, tab);
       }
     }
 #pragma unroll
@@ -1480,7 +1480,7 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
   const SwSweep& sw = plan.sweeps[k];
   const int ns = sw.s1 - sw.s0;
   if (ns < 1 || ns > kSweepMaxStages || sw.nr > SW_MAX_NR) return false;
-  const int g_lo = plan.stages[sw.s0].g0, g_hi = plan.stages[sw.s1 - 1].g1;
+  const int g_lo = sweep_first_gate(plan, sw), g_hi = plan.stages[sw.s1 - 1].g1;
   if (g_hi - g_lo > kSweepMaxGates) return false;
   p->tm_rank = 0;
   p->stall_first = 0;
@@ -1562,11 +1562,30 @@ bool fill_params(const Plan& plan, size_t k, SweepParams<R>* p, bool exchange_sw
       }
     }
     SwStageTab& tb = p->tabs[s];
-    tb.xm = (n_other == 0 && n_rot == 1) ? (plan.gates[rot_g].b & (nv - 1)) : 0;
+    tb.xm = (int8_t)((n_other == 0 && n_rot == 1) ? (plan.gates[rot_g].b & (nv - 1)) : 0);
     tb.pad = 0;
+    // register j reads the amplitude of register sigma(j ^ xm) of the plain read: the
+    // stage's entry folds, then the folded leading X of its rotation record
+    const StageEntry en = plan.entry.empty() ? StageEntry() : plan.entry[sw.s0 + s];
     for (int j = 0; j < 16; ++j) {
-      const int jx = j < nv ? j ^ tb.xm : j;
+      const int jx = j < nv ? en.rperm[j ^ tb.xm] : j;
+      if (jx < 0 || jx >= 16) return false;
       tb.rd[j] = s == 0 ? off[jx] : (uint16_t)apply_swizzle(off[jx], zin[s], K);
+    }
+    for (int k = 0; k < 2; ++k) {
+      tb.rf_g[k] = -1;
+      tb.rf_off[k] = 0;
+      if (k >= en.n_rf) continue;
+      if (en.rf_g[k] < g_lo || en.rf_g[k] >= g_hi || en.rf_d[k] <= 0 || en.rf_d[k] >= nv)
+        return false;
+      tb.rf_g[k] = (int8_t)(en.rf_g[k] - g_lo);
+      tb.rf_off[k] = s == 0 ? off[en.rf_d[k]] : (uint16_t)apply_swizzle(off[en.rf_d[k]], zin[s], K);
+    }
+    if (s == 0) {
+      for (int j = 0; j < 16; ++j)
+        p->gread0[j] = host_spread(off[j < nv ? en.rperm[j ^ tb.xm] : j], sw);
+      for (int k = 0; k < 2; ++k)
+        p->rf_goff0[k] = k < en.n_rf ? host_spread(off[en.rf_d[k]], sw) : 0u;
     }
     for (int j = 0; j < 16; ++j) {
       const int pj = (j < nv) ? st.perm[j] : j;
@@ -1646,8 +1665,11 @@ bool check_exchanges_t(const Plan& plan, int64_t* st) {
           const uint32_t b = br ^ p.tabs[s].rd[j];
           if (a >= (1u << T) || b >= (1u << T) || wslot[a] >= 0 || rslot[b] >= 0) return false;
           wslot[a] = lw | off_of(sw, sw.perm[j]);
-          // register j takes the amplitude of register j ^ xm (the folded leading X)
-          rslot[b] = lr | off_of(sr, j ^ p.tabs[s].xm);
+          // register j takes the amplitude of register sigma(j ^ xm) (the stage's
+          // entry folds and the folded leading X)
+          const int jr = plan.entry.empty() ? (j ^ p.tabs[s].xm)
+                                            : plan.entry[plan.sweeps[k].s0 + s].rperm[j ^ p.tabs[s].xm];
+          rslot[b] = lr | off_of(sr, jr);
         }
         for (int a = 0; a < nr; ++a)
           if (p.tabs[s - 1].xoff[a] != slot_of(1u << sw.R[a], p.tabs[s])) return false;
@@ -1765,7 +1787,7 @@ bool adjoint_plan_supported(const Plan& plan) {
   for (const SwSweep& sw : plan.sweeps) {
     if (sw.nr != 3 || sw.T - sw.nr < 5 || sw.T - sw.nr > 8 || sw.relayout) return false;
     if (!(sw.scale_re == 1.0 && sw.scale_im == 0.0)) return false;
-    for (int g = plan.stages[sw.s0].g0; g < plan.stages[sw.s1 - 1].g1; ++g) {
+    for (int g = sweep_first_gate(plan, sw); g < plan.stages[sw.s1 - 1].g1; ++g) {
       switch (plan.gates[g].kind) {
         case SK_G1: case SK_X: case SK_SWAP: case SK_D1: case SK_D2: case SK_DP:
         case SK_CX: case SK_DPR: case SK_G1ALL: case SK_D1R: case SK_X0: case SK_CX0: case SK_DTAB:
@@ -1804,7 +1826,13 @@ cudaError_t launch_adjoint_t(void* psi, void* lam, const Plan& plan, size_t k, d
   // 256-thread tiles at two CTAs per SM (128 registers); smaller tiles at three
   // (170 registers: the two states' registers without spills)
   const size_t smem = 2 * (sizeof(A) << p.T) + sizeof(double) * (size_t)n_probes * (threads / 32);
-  auto kern = threads == 256 ? k_adjoint_sweep<R, 3, 256, 2> : k_adjoint_sweep<R, 3, 128, 3>;
+  // the lite record switch when every record of the sweep is one of its kinds
+  bool lite = true;
+  for (int st = 0; st < p.n_stages; ++st)
+    for (int g = p.stages[st].g0; g < p.stages[st].g1; ++g) lite = lite && adjoint_lite_kind(p.gates[g].kind);
+  if (const char* v = getenv("STATECRAFT_B200_ADJOINT_LITE")) lite = lite && atoi(v) != 0;
+  auto kern = threads == 256 ? (lite ? k_adjoint_sweep<R, 3, 256, 2, true> : k_adjoint_sweep<R, 3, 256, 2, false>)
+                             : (lite ? k_adjoint_sweep<R, 3, 128, 3, true> : k_adjoint_sweep<R, 3, 128, 3, false>);
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)smem);
   if (e != cudaSuccess) return e;

@@ -614,6 +614,51 @@ std::vector<SwPerm> restore_identity(const int* phys_in, int n) {
 
 }  // namespace
 
+// Entry folds (StageEntry): the records that open stage st and only permute its
+// registers are taken out of its range and composed into the read.  Record i acts as
+// new v[j] = old v[pi_i(j)]; after the prefix, v[j] = read[sigma(j)] with
+// sigma = pi_1 o pi_2 o ...  A conditional X on register bit a (controls outside the
+// registers) translates by e_a where its condition holds, which moves sigma's
+// result by the linear part of the composition so far applied to e_a (rf_d).
+void fold_stage_entry(const Plan& plan, SwStage& st, StageEntry* en) {
+  const int nv = 1 << st.nr;
+  uint32_t regpos = 0;
+  for (int k = 0; k < st.nr; ++k) regpos |= 1u << st.R[k];
+  int sigma[16];
+  for (int j = 0; j < 16; ++j) sigma[j] = j;
+  int g = st.g0;
+  for (; g < st.g1; ++g) {
+    const SwGate& q = plan.gates[g];
+    int pi[16];
+    for (int j = 0; j < 16; ++j) pi[j] = j;
+    const bool plain = q.lmask == 0 && q.gmask == 0;
+    if (plain && q.kind == SK_X0) {
+      for (int j = 0; j < nv; ++j) pi[j] = j ^ (1 << q.a);
+    } else if (plain && q.kind == SK_CX0) {
+      for (int j = 0; j < nv; ++j) pi[j] = ((j >> q.b) & 1) ? j ^ (1 << q.a) : j;
+    } else if (plain && q.kind == SK_SWAP) {
+      for (int j = 0; j < nv; ++j) {
+        const int ba = (j >> q.a) & 1, bb = (j >> q.b) & 1;
+        pi[j] = ba == bb ? j : j ^ ((1 << q.a) | (1 << q.b));
+      }
+    } else if ((q.kind == SK_X0 || q.kind == SK_X) && !(q.lmask & regpos) &&
+               en->n_rf < kEntryMaxCond) {
+      // the translation's delta through the linear part of sigma
+      en->rf_g[en->n_rf] = g;
+      en->rf_d[en->n_rf] = sigma[1 << q.a] ^ sigma[0];
+      ++en->n_rf;
+      continue;
+    } else {
+      break;
+    }
+    int nsig[16];
+    for (int j = 0; j < 16; ++j) nsig[j] = j < nv ? sigma[pi[j]] : j;
+    for (int j = 0; j < 16; ++j) sigma[j] = nsig[j];
+  }
+  for (int j = 0; j < 16; ++j) en->rperm[j] = (int8_t)sigma[j];
+  st.g0 = g;
+}
+
 Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
   Plan plan;
   const int G = (int)gates.size();
@@ -1233,7 +1278,11 @@ Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp) {
       merge_register_diagonals(plan, st.g0, NR, (size_t)sw.pool0 + (size_t)pp.max_pool);
       plan.gate_ops.insert(plan.gate_ops.end(), folded_ops.begin(), folded_ops.end());
       st.g1 = (int32_t)plan.gates.size();
+      StageEntry en;
+      en.g_start = st.g0;
+      if (pp.entry_fold) fold_stage_entry(plan, st, &en);
       plan.stages.push_back(st);
+      plan.entry.push_back(en);
     }
     sw.s1 = (int32_t)plan.stages.size();
     sw.pool1 = (int32_t)plan.pool.size();

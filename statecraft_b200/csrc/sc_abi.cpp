@@ -257,6 +257,7 @@ PlanParams Ctx::plan_params() const {
   pp.rot_min_c = rotation ? (c64 ? 0.25 : 0.05) : 0.0;
   pp.scale_floor = c64 ? 0x1p-30 : 0x1p-200;
   pp.peephole = peephole;
+  pp.entry_fold = entry_fold;
   return pp;
 }
 
@@ -318,11 +319,44 @@ int Ctx::apply_gates(const std::vector<PGate>& gates) {
   return apply_sweeps(gates);
 }
 
+namespace {
+
+bool same_plan_params(const PlanParams& a, const PlanParams& b) {
+  return a.tile_qubits == b.tile_qubits && a.low_qubits == b.low_qubits && a.nr == b.nr &&
+         a.budget == b.budget && a.max_gates == b.max_gates && a.max_pool == b.max_pool &&
+         a.relayout == b.relayout && a.rot_min_c == b.rot_min_c &&
+         a.scale_floor == b.scale_floor && a.peephole == b.peephole &&
+         a.entry_fold == b.entry_fold && a.phase_free == b.phase_free;
+}
+
+bool same_gates(const std::vector<PGate>& a, const std::vector<PGate>& b) {
+  if (a.size() != b.size()) return false;
+  for (size_t i = 0; i < a.size(); ++i) {
+    const PGate &x = a[i], &y = b[i];
+    if (x.kind != y.kind || x.q0 != y.q0 || x.q1 != y.q1 || x.cmask != y.cmask ||
+        x.op_index != y.op_index || std::memcmp(x.m, y.m, sizeof x.m) != 0)
+      return false;
+  }
+  return true;
+}
+
+}  // namespace
+
 int Ctx::apply_sweeps(const std::vector<PGate>& gates) {
   if (gates.empty()) return SC_OK;
   const double amp_bytes = (cfg.dtype == SC_C64) ? 8.0 : 16.0;
   const double dim = std::ldexp(1.0, n);
-  Plan plan = plan_sweeps(gates, n, plan_params());
+  const PlanParams pp = plan_params();
+  if (!(plan_cache_valid && plan_cache_n == n && same_plan_params(plan_cache_pp, pp) &&
+        same_gates(plan_cache_gates, gates))) {
+    plan_cache_valid = false;
+    plan_cache = plan_sweeps(gates, n, pp);
+    plan_cache_gates = gates;
+    plan_cache_n = n;
+    plan_cache_pp = pp;
+    plan_cache_valid = plan_cache.ok;
+  }
+  const Plan& plan = plan_cache;
   if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
   for (size_t k = 0; k < plan.sweeps.size(); ++k) {
     mark_begin(KC_SWEEP, 2.0 * dim * amp_bytes);
@@ -518,6 +552,7 @@ int32_t sc_create(int32_t device, const sc_config* cfg, void** out_ctx) {
   if (const char* v = getenv("STATECRAFT_B200_RELAYOUT")) c->relayout = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_ROTATION")) c->rotation = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_PEEPHOLE")) c->peephole = atoi(v) != 0;
+  if (const char* v = getenv("STATECRAFT_B200_ENTRY_FOLD")) c->entry_fold = atoi(v) != 0;
   if (const char* v = getenv("STATECRAFT_B200_ADJOINT_FUSED")) c->adjoint_fused = atoi(v) != 0;
   // minimum sweep-path cost of a dense block (FMA per amplitude); 0 turns blocks off
   if (const char* v = getenv("STATECRAFT_B200_DENSE_BLOCKS")) c->dense_block_cost = atof(v);

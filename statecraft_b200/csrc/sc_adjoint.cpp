@@ -136,6 +136,7 @@ PlanParams reverse_plan_params(const Ctx* c) {
   // both states take every gate: phases common to a gate cancel in the probes, so
   // real rotations run as lifting shears and 1-qubit diagonals as diag(1, d)
   pp.phase_free = true;
+  pp.entry_fold = c->entry_fold;
   return pp;
 }
 

@@ -42,10 +42,20 @@ struct Ctx {
   bool relayout = true;
   bool rotation = true;  // rotation form for 1-qubit unitaries in sweeps
   bool peephole = true;  // per-stage record peephole in the planner
+  bool entry_fold = true;  // register permutations opening a stage folded into its read
   bool adjoint_fused = true;  // adjoint reverse pass as dual-state sweeps when it fits
   // runs of gates on <= 5 qubits whose sweep-path cost (FMA per amplitude) reaches this
   // become dense tensor-core blocks (complex128; 0 = never)
   double dense_block_cost = 160.0;
+
+  // The plan of the last fused gate list (apply_sweeps), reused when the next run
+  // plans the same gates on the same qubit count with the same settings: a circuit
+  // simulated again (new seeds, new shots) skips the host planner.
+  std::vector<PGate> plan_cache_gates;
+  int plan_cache_n = -1;
+  PlanParams plan_cache_pp{};
+  Plan plan_cache;
+  bool plan_cache_valid = false;
 
   // state
   int n = 0;

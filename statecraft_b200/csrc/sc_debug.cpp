@@ -30,6 +30,7 @@ PlanParams debug_params(int tile, int low, int nr, double budget) {
   pp.rot_min_c = 0.05;
   if (const char* v = getenv("STATECRAFT_B200_ROTATION")) pp.rot_min_c = atoi(v) != 0 ? 0.05 : 0.0;
   if (const char* v = getenv("STATECRAFT_B200_PEEPHOLE")) pp.peephole = atoi(v) != 0;
+  if (const char* v = getenv("STATECRAFT_B200_ENTRY_FOLD")) pp.entry_fold = atoi(v) != 0;
   return pp;
 }
 
@@ -84,7 +85,7 @@ inline C mac2(const double* m0, C a0, const double* m1, C a1) {
 void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
                    const uint8_t* codes = nullptr) {
   // the kernel sees only the sweep's pool range: a record outside it poisons the state
-  for (int gi = plan.stages[sw.s0].g0; gi < plan.stages[sw.s1 - 1].g1; ++gi)
+  for (int gi = sweep_first_gate(plan, sw); gi < plan.stages[sw.s1 - 1].g1; ++gi)
     if (plan.gates[gi].moff < sw.pool0 || plan.gates[gi].moff > sw.pool1) {
       for (uint64_t e = 0; e < 2ULL * (uint64_t)sw.tiles << sw.T; ++e) st[e] = std::nan("");
       return;
@@ -121,8 +122,16 @@ void emulate_sweep(double* st, const Plan& plan, const SwSweep& sw,
           for (int k = 0; k < NR; ++k)
             if (j & (1 << k)) o |= 1u << stg.R[k];
           off[j] = o;
-          v[j] = tb[l0 | o];
         }
+        // entry folds: register j reads register rperm[j] of the plain read, flipped
+        // by rf_d[k] where the condition of the folded record rf_g[k] holds
+        int rflip = 0;
+        const StageEntry en = plan.entry.empty() ? StageEntry() : plan.entry[s];
+        for (int k = 0; k < en.n_rf; ++k) {
+          const SwGate& q = plan.gates[en.rf_g[k]];
+          if ((base & q.gmask) == q.gmask && (l0 & q.lmask) == q.lmask) rflip ^= en.rf_d[k];
+        }
+        for (int j = 0; j < NV; ++j) v[j] = tb[l0 | off[en.rperm[j] ^ rflip]];
         for (int gi = stg.g0; gi < stg.g1; ++gi) {
           const SwGate& g = plan.gates[gi];
           if ((base & g.gmask) != g.gmask) continue;

@@ -197,6 +197,8 @@ struct PlanParams {
   double scale_floor = 0x1p-200;
   // per-stage record peephole (diagonals merged or moved, permutations folded)
   bool peephole = true;
+  // fold the register permutations that open a stage into its read (StageEntry)
+  bool entry_fold = true;
   // a common phase of the whole state may be dropped: the adjoint reverse pass
   // applies every gate to both of its states, so a phase e^{ig} (or a sign) on a
   // gate cancels in every probe Im <lambda| P |psi>.  1-qubit real rotations up to
@@ -207,9 +209,29 @@ struct PlanParams {
 // matrix reals a normalised gate stores in the sweep pool
 int gate_pool_size(const PGate& g);
 
+// Entry folds of a stage (host side): the register permutations that open a stage
+// (X, CNOT and SWAP on register bits, and X on a register bit controlled from outside
+// the registers) are not executed as records but folded into the stage's read: the
+// thread's register j reads the amplitude of register rperm[j] of the plain read,
+// with register-index flip rf_d[k] where the condition of record rf_g[k] holds (its
+// global controls gmask on the tile, its tile-position controls lmask on the thread).
+// The folded records stay in `gates` just before the stage's range (g_start .. g0).
+constexpr int kEntryMaxCond = 2;
+struct StageEntry {
+  int32_t g_start = 0;  // the stage's first record before folding
+  int8_t rperm[16];
+  int32_t n_rf = 0;
+  int32_t rf_g[kEntryMaxCond] = {-1, -1};
+  int32_t rf_d[kEntryMaxCond] = {0, 0};
+  StageEntry() {
+    for (int j = 0; j < 16; ++j) rperm[j] = (int8_t)j;
+  }
+};
+
 struct Plan {
   std::vector<SwSweep> sweeps;
   std::vector<SwStage> stages;
+  std::vector<StageEntry> entry;  // per stage (empty: no entry folds)
   std::vector<SwGate> gates;
   std::vector<double> pool;
   std::vector<int64_t> gate_ops;  // host only: op index of each entry of `gates`
@@ -220,6 +242,11 @@ struct Plan {
 
 // Builds the sweep plan for a gate list on n qubits.
 Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp);
+
+// First record of sweep k (entry folds included) and of stage s.
+inline int32_t sweep_first_gate(const Plan& plan, const SwSweep& sw) {
+  return plan.entry.empty() ? plan.stages[sw.s0].g0 : plan.entry[sw.s0].g_start;
+}
 
 
 // ---------------------------------------------------------------------------

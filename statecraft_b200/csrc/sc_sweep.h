@@ -26,13 +26,18 @@ constexpr int kSweepMaxPool = 2048;  // matrix reals
 // read bits >= K, so every swizzle is a bijection and XOR-linear over disjoint bits.
 // rows[] here is the swizzle of the layout this stage reads; bit 15 of rows[0]
 // marks one that differs from the fixed default (rows[k] = 1 << (K + k)).
+// Entry folds (StageEntry in the plan) are already in rd[]; their conditional part:
+// where the condition of record rf_g[k] (its gmask on the tile, its lmask on the
+// thread) holds, the thread's read slots are XORed with rf_off[k] (rf_g[k] < 0: none).
 struct SwStageTab {
   uint16_t rd[16];
   uint16_t wsoff[16];
   uint16_t xoff[4];
   uint16_t rows[4];
-  int32_t xm;
-  int32_t pad;
+  int8_t xm;
+  int8_t rf_g[2];
+  int8_t pad;
+  uint16_t rf_off[2];
 };
 
 // Whole-tile bulk tensor copies (TMA).  The state is described to the copy engine
@@ -72,6 +77,8 @@ struct SweepParams {
   uint8_t outp[32];         // physical bit of tile position p in the output layout
   uint16_t off0[16];     // tile offset of register j in the first stage (linear layout)
   uint32_t gfirst[16];   // global offset of register j in the first stage's layout
+  uint32_t gread0[16];   // global offset register j reads in the first stage (entry folds applied)
+  uint32_t rf_goff0[2];  // the first stage's conditional entry flips as global offsets
   uint32_t glast[16];    // global offset register j is stored to (last stage, perm applied)
   uint16_t lastoff[16];  // tile offset register j is stored to (last stage, perm applied)
   R scale_re, scale_im;  // applied to every amplitude at the store (rotation-form scalars)
