@@ -1094,22 +1094,73 @@ __global__ void __launch_bounds__(THREADS, MINB)
         const SwGate& g = p.gates[gi];
         if (((uint64_t)base & g.gmask) != g.gmask) continue;
         if (g.kind == SK_PROBE) {
-          double ps = 0.0;
-          switch (g.code & 15) {
+          // Up to four consecutive probes (one point of the plan: the probes of a
+          // run of rotations) are summed and then reduced over the warp together,
+          // their shuffle trees interleaved instead of one after another.
+          auto probe = [&](const SwGate& q) -> double {
+            double ps = 0.0;
+            switch (q.code & 15) {
 #define SC_PROBE_CASE(A, P)                      \
   case ((A) << 2) | (P):                         \
     if constexpr ((A) < NR) ps = probe_sum<R, NR, (A), (P)>(v, w); \
     break;
-            SC_PROBE_CASE(0, 1) SC_PROBE_CASE(0, 2) SC_PROBE_CASE(0, 3)
-            SC_PROBE_CASE(1, 1) SC_PROBE_CASE(1, 2) SC_PROBE_CASE(1, 3)
-            SC_PROBE_CASE(2, 1) SC_PROBE_CASE(2, 2) SC_PROBE_CASE(2, 3)
-            SC_PROBE_CASE(3, 1) SC_PROBE_CASE(3, 2) SC_PROBE_CASE(3, 3)
+              SC_PROBE_CASE(0, 1) SC_PROBE_CASE(0, 2) SC_PROBE_CASE(0, 3)
+              SC_PROBE_CASE(1, 1) SC_PROBE_CASE(1, 2) SC_PROBE_CASE(1, 3)
+              SC_PROBE_CASE(2, 1) SC_PROBE_CASE(2, 2) SC_PROBE_CASE(2, 3)
+              SC_PROBE_CASE(3, 1) SC_PROBE_CASE(3, 2) SC_PROBE_CASE(3, 3)
 #undef SC_PROBE_CASE
-            default: break;
+              default: break;
+            }
+            return ps;
+          };
+          // the next record joins the group when it is a probe (probes carry no
+          // global controls)
+          auto next_probe = [&]() {
+            return gi + 1 < stg.g1 && p.gates[gi + 1].kind == SK_PROBE && p.gates[gi + 1].gmask == 0;
+          };
+          double p0 = probe(g), p1 = 0.0, p2 = 0.0, p3 = 0.0;
+          const uint32_t b0 = (uint32_t)g.b;  // b: local probe index
+          uint32_t b1 = 0, b2 = 0, b3 = 0;
+          int np = 1;
+          if (next_probe()) {
+            ++gi;
+            p1 = probe(p.gates[gi]);
+            b1 = (uint32_t)p.gates[gi].b;
+            np = 2;
+            if (next_probe()) {
+              ++gi;
+              p2 = probe(p.gates[gi]);
+              b2 = (uint32_t)p.gates[gi].b;
+              np = 3;
+              if (next_probe()) {
+                ++gi;
+                p3 = probe(p.gates[gi]);
+                b3 = (uint32_t)p.gates[gi].b;
+                np = 4;
+              }
+            }
           }
+          if (np <= 2) {
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) ps += __shfl_xor_sync(0xffffffffu, ps, o);
-          if ((tid & 31u) == 0) acc[(uint32_t)g.b * nwarps + warp] += ps;  // b: local probe index
+            for (int o = 16; o > 0; o >>= 1) {
+              p0 += __shfl_xor_sync(0xffffffffu, p0, o);
+              p1 += __shfl_xor_sync(0xffffffffu, p1, o);
+            }
+          } else {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+              p0 += __shfl_xor_sync(0xffffffffu, p0, o);
+              p1 += __shfl_xor_sync(0xffffffffu, p1, o);
+              p2 += __shfl_xor_sync(0xffffffffu, p2, o);
+              p3 += __shfl_xor_sync(0xffffffffu, p3, o);
+            }
+          }
+          if ((tid & 31u) == 0) {
+            acc[b0 * nwarps + warp] += p0;
+            if (np > 1) acc[b1 * nwarps + warp] += p1;
+            if (np > 2) acc[b2 * nwarps + warp] += p2;
+            if (np > 3) acc[b3 * nwarps + warp] += p3;
+          }
           continue;
         }
         apply_record_pair<R, NR, kLite>(v, w, g, p.pool + g.moff, l0, off, base, bp, bl, rbase, tab);
