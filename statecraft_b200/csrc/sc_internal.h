@@ -243,7 +243,7 @@ struct Plan {
 // Builds the sweep plan for a gate list on n qubits.
 Plan plan_sweeps(const std::vector<PGate>& gates, int n, const PlanParams& pp);
 
-// First record of sweep k (entry folds included) and of stage s.
+// First record of a sweep, the records its first stage folded into its read included.
 inline int32_t sweep_first_gate(const Plan& plan, const SwSweep& sw) {
   return plan.entry.empty() ? plan.stages[sw.s0].g0 : plan.entry[sw.s0].g_start;
 }

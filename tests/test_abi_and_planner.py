@@ -390,3 +390,22 @@ def test_tile_tensor_boxes_match_tile_enumeration(dtype):
         assert rc > 0, A.load().sc_last_error()
         boxed += int(stats[0])
     assert boxed > 10
+
+
+@pytest.mark.parametrize("fold", ["0", "1"])
+@pytest.mark.parametrize("cfg", [(11, 4, 3, -1.0), (10, 4, 4, -1.0), (9, 3, 2, -1.0)])
+def test_entry_folds_match_oracle(fold, cfg, monkeypatch):
+    """Register permutations that open a stage are folded into its read (X, CNOT,
+    SWAP, and X controlled from outside the registers, with per-thread flips); the
+    emulated plan matches the oracle with the folds on and off, on circuits made of
+    permutations between rotation layers."""
+    monkeypatch.setenv("STATECRAFT_B200_ENTRY_FOLD", fold)
+    tile, low, nr, budget = cfg
+    for seed in range(3):
+        n = 12
+        c = RCirc.random_circuit(n, 120, seed=500 + seed,
+                                 kinds=["single", "cnot", "swap", "multi", "cnot", "cnot"])
+        init = RCirc.random_state(n, seed)
+        got, _ = _emulate(c, init, tile, low, nr, budget)
+        want = _oracle(c, init)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12)
