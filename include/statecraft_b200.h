@@ -262,6 +262,11 @@ SC_API int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, i
                             int32_t low_qubits, int32_t nr, double budget, int64_t* order,
                             int64_t* n_sweeps, int64_t* n_stages, int64_t* n_relayouts,
                             int64_t* n_restores);
+/* Entry folds of the plan of ops: stats[3] = {stages, records folded into a stage's
+ * read (register permutations opening a stage), of which conditional (an X with
+ * controls outside the registers, applied as a per-thread read flip)}. */
+SC_API int32_t sc_debug_entry_folds(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                                    int32_t low_qubits, int32_t nr, double budget, int64_t* stats);
 /* Executes the sweep plan on a host complex128 state (interleaved doubles) with the
  * kernel's tile / stage / register semantics; returns the number of sweeps. */
 SC_API int32_t sc_debug_emulate_sweeps(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,

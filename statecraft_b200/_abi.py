@@ -145,6 +145,9 @@ SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "sc_last_plan_stats": (ctypes.c_int32, [ctypes.c_void_p, _P(ctypes.c_int64),
                                             _P(ctypes.c_int64), _P(ctypes.c_int64)]),
+    "sc_debug_entry_folds": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
+                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                              ctypes.c_double, _P(ctypes.c_int64)]),
     "sc_debug_plan_order": (ctypes.c_int32, [ctypes.c_int32, _P(ScOp), ctypes.c_int64,
                                              ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                                              ctypes.c_double, _P(ctypes.c_int64),

@@ -353,6 +353,23 @@ void emulate_permute(double* st, int n, const SwPerm& pm) {
 
 extern "C" {
 
+int32_t sc_debug_entry_folds(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
+                             int32_t low_qubits, int32_t nr, double budget, int64_t* stats) {
+  std::vector<PGate> gates;
+  int rc = normalise_all(n, ops, n_ops, gates);
+  if (rc != SC_OK) return rc;
+  if (!stats) return fail(SC_EINVAL, "stats[3] is required");
+  Plan plan = plan_sweeps(gates, n, debug_params(tile_qubits, low_qubits, nr, budget));
+  if (!plan.ok) return fail(SC_ECUDA, "fusion planner could not stage every gate");
+  stats[0] = (int64_t)plan.stages.size();
+  stats[1] = stats[2] = 0;
+  for (size_t s = 0; s < plan.entry.size(); ++s) {
+    stats[1] += plan.stages[s].g0 - plan.entry[s].g_start;
+    stats[2] += plan.entry[s].n_rf;
+  }
+  return SC_OK;
+}
+
 int32_t sc_debug_plan_order(int32_t n, const sc_op* ops, int64_t n_ops, int32_t tile_qubits,
                             int32_t low_qubits, int32_t nr, double budget, int64_t* order,
                             int64_t* n_sweeps, int64_t* n_stages, int64_t* n_relayouts,

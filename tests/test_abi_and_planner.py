@@ -405,6 +405,15 @@ def test_entry_folds_match_oracle(fold, cfg, monkeypatch):
         n = 12
         c = RCirc.random_circuit(n, 120, seed=500 + seed,
                                  kinds=["single", "cnot", "swap", "multi", "cnot", "cnot"])
+        # the plan does fold: records taken into stage reads, conditional ones among them
+        ops, n_ops = serialize_circuit(c)
+        st = np.zeros(3, dtype=np.int64)
+        assert A.load().sc_debug_entry_folds(n, ops, n_ops, tile, low, nr, budget,
+                                             st.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))) == A.SC_OK
+        if fold == "1":
+            assert st[1] > 0 and st[2] > 0, st
+        else:
+            assert st[1] == 0 and st[2] == 0, st
         init = RCirc.random_state(n, seed)
         got, _ = _emulate(c, init, tile, low, nr, budget)
         want = _oracle(c, init)
